@@ -1,0 +1,257 @@
+/*
+ * crmpm_b200.h — C ABI of the B200-native MPM substep engine.
+ *
+ * This library replaces CRESSim-MPM's GPU solvers (src/solver/gpu_*_mpm_solver.cu) behind the
+ * reference's own solver interface (include/solver/mpm_solver.h:63-191,
+ * src/solver/mpm_solver_base.h:41-171, src/solver/mpm_solver_gpu.h:43-57).  Every entry point
+ * below names the reference member it stands in for.  All pointers handed to a solver are DEVICE
+ * pointers unless the argument name ends in "Host"; every call is asynchronous on the solver's
+ * CUDA stream except where stated.
+ *
+ * Error convention: every function returns CRB200_OK (0) or a negative CRB200_ERR_* code and
+ * records a message readable with CrB200GetLastError().  The reference logs CUDA errors and
+ * continues (src/utils/check_cuda.cuh:35-44); this library reports them instead.
+ *
+ * The struct layouts below are field-for-field the layouts of the reference's SoA descriptors so
+ * that a reference-side adapter can pass its own structs by reinterpretation:
+ *   CrB200ShapeData       == crmpm::ShapeData        (include/engine/shape.h:58-89)
+ *   CrB200GeometryData    == crmpm::GeometryData     (include/engine/geometry.h:65-108)
+ *   CrB200GeometrySdfData == crmpm::GeometrySdfData  (include/engine/geometry.h:113-118)
+ * Vec3f and Quat are 16-byte float4 in the reference (include/math/vec3.h:388-396,
+ * include/math/quat.h:48-56); they appear here as CrB200Float4.
+ */
+#ifndef CRMPM_B200_H
+#define CRMPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CRB200_API __attribute__((visibility("default")))
+#else
+#define CRB200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ */
+/* Status codes                                                                                */
+/* ------------------------------------------------------------------------------------------ */
+
+#define CRB200_OK 0
+#define CRB200_ERR_INVALID_ARGUMENT (-1)
+#define CRB200_ERR_NOT_INITIALIZED (-2)
+#define CRB200_ERR_UNSUPPORTED (-3)
+#define CRB200_ERR_CUDA (-4)
+#define CRB200_ERR_OUT_OF_MEMORY (-5)
+#define CRB200_ERR_CAPACITY (-6)
+#define CRB200_ERR_TIMEOUT (-7)
+#define CRB200_ERR_NUMERICS (-8)
+
+/* Device status word bits, see CrB200SolverGetStatus(). */
+#define CRB200_STATUS_NAN_STATE 0x1u      /* NaN/Inf found in particle position or velocity */
+#define CRB200_STATUS_BLOCK_OVERFLOW 0x2u /* a grid block held more particles than a tile pass */
+#define CRB200_STATUS_OUT_OF_DOMAIN 0x4u  /* a particle started a substep outside the grid     */
+
+/* MpmSolverType values (include/solver/mpm_solver.h:51-61).  Only the GPU kinds are accepted:
+ * the CPU kinds belong to the reference and have no counterpart here. */
+#define CRB200_SOLVER_GPU_MLS 1
+#define CRB200_SOLVER_GPU_PB 3
+#define CRB200_SOLVER_GPU_STANDARD 5
+
+/* ShapeContactModel (include/solver/mpm_solver.h:45-49). */
+#define CRB200_CONTACT_KINEMATIC 0
+#define CRB200_CONTACT_EFFECTIVE_MASS 1
+
+/* ParticleMaterialType (include/solver/material_data.h:44-49). */
+#define CRB200_MATERIAL_COROTATIONAL 0
+#define CRB200_MATERIAL_NEOHOOKEAN 1
+#define CRB200_MATERIAL_LINEAR_ELASTIC 2
+
+/* ShapeType (include/engine/shape.h:47-52). */
+#define CRB200_SHAPE_STATIC 0
+#define CRB200_SHAPE_KINEMATIC 1
+#define CRB200_SHAPE_DYNAMIC 2
+
+/* GeometryType (include/engine/geometry.h:41-59). */
+#define CRB200_GEOM_BOX 0
+#define CRB200_GEOM_SPHERE 1
+#define CRB200_GEOM_PLANE 2
+#define CRB200_GEOM_CAPSULE 3
+#define CRB200_GEOM_TRIANGLE_MESH 4
+#define CRB200_GEOM_QUAD_SLICER 5
+#define CRB200_GEOM_TRIANGLE_MESH_SLICER 6
+#define CRB200_GEOM_CONNECTED_LINE_SEGMENTS 7
+#define CRB200_GEOM_ARC 8
+
+/* ------------------------------------------------------------------------------------------ */
+/* Plain data descriptors                                                                      */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct CrB200Float4 { float x, y, z, w; } CrB200Float4;
+typedef struct CrB200Int4 { int x, y, z, w; } CrB200Int4;
+
+/* Rigid shapes, struct-of-arrays, indexed by global shape id (include/engine/shape.h:58-89). */
+typedef struct CrB200ShapeData {
+    int *type;                     /* CRB200_SHAPE_* */
+    int *geometryIdx;              /* geometry id of each shape */
+    CrB200Float4 *position;        /* xyz */
+    CrB200Float4 *rotation;        /* quaternion (x, y, z, w) */
+    CrB200Float4 *invScale;        /* xyz */
+    CrB200Float4 *linearVelocity;  /* xyz */
+    CrB200Float4 *angularVelocity; /* xyz */
+    CrB200Float4 *comInvMass;      /* centre of mass xyz, inverse mass w */
+    CrB200Float4 *inertiaInv0;     /* inverse inertia, diagonal */
+    CrB200Float4 *inertiaInv1;     /* inverse inertia, off-diagonal (xy, xz, yz) */
+    CrB200Float4 *force;           /* output coupling force (dynamic shapes) */
+    CrB200Float4 *torque;          /* output coupling torque (dynamic shapes) */
+    CrB200Float4 *params0;         /* x smooth distance, y drag, z friction, w SDF fatten */
+    int size;
+} CrB200ShapeData;
+
+/* Geometry, struct-of-arrays (include/engine/geometry.h:65-108). */
+typedef struct CrB200GeometryData {
+    int *type;             /* CRB200_GEOM_* */
+    CrB200Float4 *params0; /* per-type parameters, integer fields bit-cast into floats */
+    int size;
+} CrB200GeometryData;
+
+/* Precomputed SDF grids and line points (include/engine/geometry.h:113-118). */
+typedef struct CrB200GeometrySdfData {
+    CrB200Int4 *dimension;                /* per SDF id */
+    CrB200Float4 *lowerBoundCellSize;     /* per SDF id: lower bound xyz, cell size w */
+    CrB200Float4 *gradientSignedDistance; /* flattened grids: gradient xyz, distance w */
+} CrB200GeometrySdfData;
+
+typedef struct CrB200Solver *CrB200SolverHandle;
+
+/* ------------------------------------------------------------------------------------------ */
+/* Library                                                                                     */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Message of the last failing call on this thread (empty string if none). */
+CRB200_API const char *CrB200GetLastError(void);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+CRB200_API int CrB200GetVersion(void);
+
+/* Number of CUDA kernels this library launched since load (all solvers, all threads). */
+CRB200_API uint64_t CrB200GetKernelLaunchCount(void);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Solver life cycle                                                                           */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Create a solver.  Replaces the constructors GpuMlsMpmSolver(numParticles, cellSize, gridBound)
+ * (src/solver/gpu_mls_mpm_solver.cu:40-52), GpuPbMpmSolver and GpuStandardMpmSolver, including
+ * the node-count formula numNodesPerDim = int((max - min) / cellSize + 1) in float.
+ * `stream` is a cudaStream_t (NULL = legacy default stream), as MpmSolverGpu::setCudaStream
+ * (src/solver/mpm_solver_gpu.cpp:42-50). */
+CRB200_API int CrB200SolverCreate(int solverType, int numMaxParticles, float cellSize,
+                                  const float gridMin[3], const float gridMax[3], void *stream,
+                                  CrB200SolverHandle *outSolver);
+
+/* Free every device buffer the solver owns (MpmSolver release / GpuMlsMpmSolver::_release,
+ * gpu_mls_mpm_solver.cu:111-124).  Bound buffers stay owned by the caller. */
+CRB200_API int CrB200SolverRelease(CrB200SolverHandle solver);
+
+/* MpmSolver::initialize (mpm_solver.h:70; gpu_mls_mpm_solver.cu:54-83): allocate solver-owned
+ * state for numMaxParticles and zero it.  Particle data must be bound first. */
+CRB200_API int CrB200SolverInitialize(CrB200SolverHandle solver);
+
+/* MpmSolver::step (mpm_solver.h:75): one substep (PB-MPM: one step of `iterations` solver
+ * iterations plus integration).  Writes the integration step size to *outDt (may be NULL). */
+CRB200_API int CrB200SolverStep(CrB200SolverHandle solver, float *outDt);
+
+/* Run `numSteps` steps back to back (the reference's `while (t < dt) t += step()` loop body
+ * repeated, src/engine/scene_impl.cpp:313-317) without host round trips. */
+CRB200_API int CrB200SolverStepMany(CrB200SolverHandle solver, int numSteps);
+
+/* MpmSolver::fetchResults (mpm_solver_gpu.cpp:37-40): wait for the solver stream. */
+CRB200_API int CrB200SolverFetchResults(CrB200SolverHandle solver);
+
+/* MpmSolver::computeInitialData (mpm_solver.h:86-87; gpu_mls_mpm_solver.cu:85-100): F = I and
+ * initial volume V0 = m / (sum_n w * m_n / dx^3) for the listed particles.  `indicesDevice` holds
+ * `numParticles` particle indices in device memory. */
+CRB200_API int CrB200SolverComputeInitialData(CrB200SolverHandle solver, unsigned int numParticles,
+                                              const unsigned int *indicesDevice);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Setters and binders (MpmSolver, mpm_solver.h:80-184; MpmSolverBase, mpm_solver_base.h)      */
+/* ------------------------------------------------------------------------------------------ */
+
+CRB200_API int CrB200SolverSetGravity(CrB200SolverHandle solver, float gx, float gy, float gz);
+CRB200_API int CrB200SolverSetIntegrationStepSize(CrB200SolverHandle solver, float dt);
+CRB200_API int CrB200SolverSetSolverIterations(CrB200SolverHandle solver, int iterations);
+CRB200_API int CrB200SolverSetShapeContactModel(CrB200SolverHandle solver, int contactModel);
+CRB200_API int CrB200SolverSetNumActiveParticles(CrB200SolverHandle solver, unsigned int n);
+
+/* bindParticleData (mpm_solver.h:101): positionMass float4[numMaxParticles] (xyz position,
+ * w mass) and velocity float4[numMaxParticles] (xyz).  Both device pointers, 16-byte aligned. */
+CRB200_API int CrB200SolverBindParticleData(CrB200SolverHandle solver, CrB200Float4 *positionMass,
+                                            CrB200Float4 *velocity);
+
+/* bindParticleMaterials (mpm_solver.h:108): params0 float4 (x lambda, y mu for MLS/standard;
+ * x elastic relaxation, y elasticity ratio for PB-MPM) and type int (CRB200_MATERIAL_*). */
+CRB200_API int CrB200SolverBindParticleMaterials(CrB200SolverHandle solver, CrB200Float4 *params0,
+                                                 int *type);
+
+/* bindActiveMask (mpm_solver.h:125): uint8 per particle, nonzero = active. */
+CRB200_API int CrB200SolverBindActiveMask(CrB200SolverHandle solver, unsigned char *activeMask);
+
+CRB200_API int CrB200SolverSetNumShapes(CrB200SolverHandle solver, int numShapes);
+CRB200_API int CrB200SolverBindShapeIds(CrB200SolverHandle solver, int *shapeIds);
+CRB200_API int CrB200SolverBindShapeData(CrB200SolverHandle solver, const CrB200ShapeData *shapes);
+CRB200_API int CrB200SolverBindGeometryData(CrB200SolverHandle solver,
+                                            const CrB200GeometryData *geometries);
+CRB200_API int CrB200SolverBindGeometrySdfData(CrB200SolverHandle solver,
+                                               const CrB200GeometrySdfData *sdf);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Introspection (no reference counterpart; the reference keeps F, C and V0 private)           */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Grid node counts per dimension, as the reference computes them. */
+CRB200_API int CrB200SolverGetGridDims(CrB200SolverHandle solver, int outDims[3]);
+
+/* Copy solver-owned particle state for particles [0, n) to device buffers (any may be NULL):
+ * F and C as float[n*9] column-major per particle (F(r,c) at 3*c + r), V0 as float[n]. */
+CRB200_API int CrB200SolverCopyParticleState(CrB200SolverHandle solver, unsigned int n, float *F,
+                                             float *C, float *V0);
+
+/* Overwrite solver-owned particle state for particles [0, n) from device buffers (any may be
+ * NULL; same layouts as CrB200SolverCopyParticleState). */
+CRB200_API int CrB200SolverSetParticleState(CrB200SolverHandle solver, unsigned int n,
+                                            const float *F, const float *C, const float *V0);
+
+/* Sort products of the most recent substep: per-particle block key (uint32, key of an inactive
+ * particle is 0xFFFFFFFF) and the canonical permutation (particle ids ordered by key, ties by
+ * id) of the `*outNumSorted` binned particles.  Device buffers of numMaxParticles entries. */
+CRB200_API int CrB200SolverCopySortState(CrB200SolverHandle solver, unsigned int *keys,
+                                         unsigned int *sortedIds, unsigned int *outNumSortedHost);
+
+/* Slicer cut masks of the most recent substep (bit i*9 + j*3 + k set when particle and stencil
+ * node (i, j, k) lie on different sides of a slicer; mls_mpm_algorithm.h:200-210).  Device
+ * buffer of numMaxParticles uint32.  Fails with CRB200_ERR_UNSUPPORTED unless cut masks are on. */
+CRB200_API int CrB200SolverCopyCutMasks(CrB200SolverHandle solver, unsigned int *masks);
+
+/* Sticky device status word (CRB200_STATUS_*), read with a bounded wait of timeoutMs
+ * milliseconds on the solver stream; returns CRB200_ERR_TIMEOUT if the stream is still busy. */
+CRB200_API int CrB200SolverGetStatus(CrB200SolverHandle solver, unsigned int *outStatusHost,
+                                     int timeoutMs);
+CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
+
+/* Option switches: CRB200_OPT_DETERMINISTIC orders every floating-point reduction so that two
+ * runs on identical inputs give bitwise-identical outputs; CRB200_OPT_CUT_MASKS keeps the
+ * per-particle slicer masks for CrB200SolverCopyCutMasks. */
+#define CRB200_OPT_DETERMINISTIC 1
+#define CRB200_OPT_CUT_MASKS 2
+CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRMPM_B200_H */
