@@ -1,0 +1,360 @@
+"""Benchmark of the B200 MPM substep engine.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload slab|cube]
+
+Workload (default): the MLS-MPM tissue slab with a rigid probe -- 1.0 x 0.2 x 1.0 m slab, cell size
+0.01 m, 8 particles per cell with seeded jitter (1,600,000 particles), Neo-Hookean E 2e4 / nu 0.4 /
+density 1050, four side faces pinned by static box SDFs, a kinematic sphere SDF (r 0.05 m,
+friction 0.3) pressing at 0.1 m/s, dt 1e-4.  One "step" is one MLS-MPM substep.  Inputs are
+synthetic (seeded), the particle state (~350 MB) is larger than the 126 MB L2.
+
+Our arm: `value` is particle-substeps/s with all data resident on the GPU (CUDA events on the
+solver stream around K substeps replayed from a CUDA graph).  `e2e` drives the same substeps through
+the C ABI's scene-style advance (CrB200SolverAdvance): 10 substeps per call, the probe pose uploaded
+from pinned host memory before each call and the particle positions and velocities read back into
+pinned host memory after it, as the reference's Scene::advance does.
+
+Reference arm (--impl reference): the reference's own CPU solver arithmetic (oracle/_ref, built
+from the reference's headers) on the same workload, single-threaded as the reference's CPU solver
+is.  On more than one GPU, rank 0 alone runs it.
+
+Multi-GPU: one scene does not shard; N GPUs run N independent replicas (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cressim-mpm_b200"))
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int, period_ms: int = 100):
+        self.gpu = gpu_index
+        self.period = period_ms
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", f"-lms={self.period}"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def make_workload(name):
+    from crmpm_b200 import scenes
+
+    if name == "slab":
+        return scenes.tissue_slab(), "MLS-MPM tissue slab + rigid probe, 1.6M particles, 121x61x121 grid, dt 1e-4"
+    if name == "cube":
+        return scenes.cube_drop(), "MLS-MPM elastic cube drop, 4096 particles, 41^3 grid, dt 2e-4"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_reference_run(scene, steps: int, warmup: int, budget_s: float):
+    """The reference's CPU solver (oracle/_ref) on the workload: (substeps/s * particles, timed, note)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as op
+
+    if not op.ref_available():
+        return None, 0, "oracle/_ref not built"
+    r = op.RefOracle(scene)
+    r.compute_initial_data()
+    for _ in range(warmup):
+        r.step(1)
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps:
+        r.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return scene.n * done / el, done, el
+
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import crmpm_b200 as cb
+
+    cb.build_library()
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    scene, desc = make_workload(args.workload)
+    n = scene.n
+    ds = cb.DeviceScene(scene, device=dev)
+    s = ds.solver
+    stream = ds.stream
+    # warm-up (graph capture happens on the first replay)
+    ds.step(max(args.warmup, 3))
+    ds.sync()
+    st = s.grid_stats()
+    touched_nodes = st["touched_nodes"]
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    launches0 = cb.kernel_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_many(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    launches = cb.kernel_launch_count() - launches0
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, world)
+    value = world * n * args.steps / (ms_max / 1e3)
+
+    # per-kernel timing pass (CUDA events around each phase on the solver stream)
+    s.set_option(cb.OPT_PHASE_TIMING, 1)
+    s.phase_times(reset=True)
+    nprof = min(50, max(10, args.steps // 10))
+    for _ in range(nprof):
+        s.step()
+    phase_ms, nph = s.phase_times(reset=True)
+    s.set_option(cb.OPT_PHASE_TIMING, 0)
+    per_phase = {name: phase_ms[i] / max(nph, 1) for i, name in enumerate(cb.PHASES)}
+    peak, peak_kind = hbm_peak()
+    alg = {"p2g": 104.0 * n + 16.0 * touched_nodes, "g2p": 96.0 * n + 16.0 * touched_nodes,
+           "grid_update": 32.0 * touched_nodes}
+    dom = max(("p2g", "g2p", "grid_update"), key=lambda k: per_phase[k])
+    achieved = alg[dom] / (per_phase[dom] / 1e3) / 1e9
+    substep_bytes = 200.0 * n + 64.0 * touched_nodes
+    substep_gbs = substep_bytes / (ms / 1e3 / args.steps) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            with open(tfile) as f:
+                traffic = json.load(f).get(args.workload, {}).get(dom)
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI: scene-style advance with host buffers
+    frame_substeps = 10
+    frame_dt = float(np.float32(scene.dt) * frame_substeps) * 0.999
+    host_pos = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
+    host_vel = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
+    probe = scene.shapes.shape_ids[-1]
+    pose_host = torch.tensor(ds.sh["position"][probe].cpu().numpy(), pin_memory=True)
+    frames = max(3, args.steps // frame_substeps)
+    s.advance(frame_dt, host_pos.data_ptr(), host_vel.data_ptr())  # warm-up
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    sub_total = 0
+    for f_ in range(frames):
+        pose_host[1] -= 0.1 * scene.dt * frame_substeps
+        with torch.cuda.stream(stream):
+            ds.sh["position"][probe].copy_(pose_host, non_blocking=True)
+        sub_total += s.advance(frame_dt, host_pos.data_ptr(), host_vel.data_ptr())
+    torch.cuda.synchronize(dev)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * n * sub_total / e2e_s
+    h2d = 16 * frames
+    d2h = 32 * n * frames
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, done, el = cpu_reference_run(scene, steps=20, warmup=1, budget_s=25.0)
+        if v is not None:
+            cpu = {"value": v, "unit": "particle-substeps/s", "cores": 1, "kind": "reference",
+                   "sample": f"{done} MLS substeps of the same 1.6M-particle slab ({el:.1f} s) with the reference's "
+                             f"serial CPU solver arithmetic built from its own headers"}
+    status = s.status()
+    out = {
+        "metric": "particle-substeps/s (MLS-MPM 1.6M p)",
+        "value": value,
+        "unit": "particle-substeps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded jittered particles)",
+        "config": {"workload": desc, "particles": n, "grid": list(s.grid_dims()), "dt": scene.dt,
+                   "substeps_per_step": 1, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (particle state ~350 MB)", "touched_nodes": touched_nodes},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "phase_ms": per_phase, "substep_gbs_algorithmic": substep_gbs,
+                     "substep_frac": substep_gbs / peak},
+        "e2e": {"value": e2e_value, "unit": "particle-substeps/s", "h2d_bytes_per_step": h2d // frames,
+                "d2h_bytes_per_step": d2h // frames, "substeps_per_step": frame_substeps},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "status": status,
+    }
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    return out
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    scene, desc = make_workload(args.workload)
+    v, done, el = cpu_reference_run(scene, steps=args.steps, warmup=min(args.warmup, 3), budget_s=150.0)
+    if v is None:
+        return {"impl": "reference", "unavailable": "reference CPU solver driver (oracle/_ref) is not built"}
+    sample = (f"{done} of {args.steps} requested MLS substeps of the 1.6M-particle slab timed ({el:.1f} s), "
+              f"reference serial CPU solver arithmetic built from its own headers")
+    return {
+        "impl": "reference",
+        "metric": "particle-substeps/s (MLS-MPM 1.6M p)",
+        "value": v,
+        "unit": "particle-substeps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": el / max(done, 1) * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded jittered particles)",
+        "config": {"workload": desc, "particles": scene.n, "substeps_per_step": 1},
+        "cpu_baseline": {"value": v, "unit": "particle-substeps/s", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="slab", choices=["slab", "cube"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        return
+    rank, world, local = dist_setup(args.gpus)
+    out = run_ours(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

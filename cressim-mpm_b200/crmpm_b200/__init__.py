@@ -1,0 +1,407 @@
+"""Python mirror of the B200 MPM engine's C ABI (include/crmpm_b200.h).
+
+``GpuSolver`` exposes the reference solver interface (``MpmSolver``,
+include/solver/mpm_solver.h:63-191) method for method: ``initialize``, ``step``,
+``fetch_results``, ``compute_initial_data``, the setters and the ``bind_*`` calls take device
+pointers exactly like the reference's GPU solvers.  ``DeviceScene`` owns the device buffers of one
+scene (as the reference's ``SceneImpl`` does, src/engine/scene_impl.cpp:42-93) and is what tests
+and the benchmark drive.
+
+The compute path is libcrmpm_b200.so only: importing this module fails loudly if the library is
+missing, and nothing here falls back to a CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import scenes  # noqa: F401  (re-exported for convenience)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libcrmpm_b200.so")
+ROOT = os.path.dirname(PKG)
+HEADER = os.path.join(ROOT, "include", "crmpm_b200.h")
+
+OK = 0
+ERR_TIMEOUT = -7
+STATUS_NAN_STATE = 0x1
+STATUS_BLOCK_OVERFLOW = 0x2
+STATUS_OUT_OF_DOMAIN = 0x4
+OPT_DETERMINISTIC = 1
+OPT_CUT_MASKS = 2
+OPT_PHASE_TIMING = 3
+PHASES = ("sort", "p2g", "grid_update", "g2p")
+
+
+class CrmpmError(RuntimeError):
+    pass
+
+
+class ShapeDataC(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("type", "geometryIdx", "position", "rotation", "invScale",
+                                          "linearVelocity", "angularVelocity", "comInvMass", "inertiaInv0",
+                                          "inertiaInv1", "force", "torque", "params0")] + [("size", C.c_int)]
+
+
+class GeometryDataC(C.Structure):
+    _fields_ = [("type", C.c_void_p), ("params0", C.c_void_p), ("size", C.c_int)]
+
+
+class GeometrySdfDataC(C.Structure):
+    _fields_ = [("dimension", C.c_void_p), ("lowerBoundCellSize", C.c_void_p), ("gradientSignedDistance", C.c_void_p)]
+
+
+_lib = None
+
+
+def build_library(force: bool = False) -> str:
+    """Compile libcrmpm_b200.so in place (nvcc, sm_100a)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("crmpm_b200_build", os.path.join(PKG, "build.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(force=force)
+
+
+def lib() -> C.CDLL:
+    """The loaded C-ABI library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CrmpmError(f"{LIB_PATH} is missing: build it with `python cressim-mpm_b200/build.py`")
+    L = C.CDLL(LIB_PATH)
+    vp, i, u, f = C.c_void_p, C.c_int, C.c_uint, C.c_float
+    sig = {
+        "CrB200GetLastError": (C.c_char_p, []),
+        "CrB200GetVersion": (i, []),
+        "CrB200GetKernelLaunchCount": (C.c_uint64, []),
+        "CrB200SolverCreate": (i, [i, i, f, vp, vp, vp, C.POINTER(vp)]),
+        "CrB200SolverRelease": (i, [vp]),
+        "CrB200SolverInitialize": (i, [vp]),
+        "CrB200SolverStep": (i, [vp, C.POINTER(f)]),
+        "CrB200SolverStepMany": (i, [vp, i]),
+        "CrB200SolverFetchResults": (i, [vp]),
+        "CrB200SolverComputeInitialData": (i, [vp, u, vp]),
+        "CrB200SolverSetGravity": (i, [vp, f, f, f]),
+        "CrB200SolverSetIntegrationStepSize": (i, [vp, f]),
+        "CrB200SolverSetSolverIterations": (i, [vp, i]),
+        "CrB200SolverSetShapeContactModel": (i, [vp, i]),
+        "CrB200SolverSetNumActiveParticles": (i, [vp, u]),
+        "CrB200SolverBindParticleData": (i, [vp, vp, vp]),
+        "CrB200SolverBindParticleMaterials": (i, [vp, vp, vp]),
+        "CrB200SolverBindActiveMask": (i, [vp, vp]),
+        "CrB200SolverSetNumShapes": (i, [vp, i]),
+        "CrB200SolverBindShapeIds": (i, [vp, vp]),
+        "CrB200SolverBindShapeData": (i, [vp, vp]),
+        "CrB200SolverBindGeometryData": (i, [vp, vp]),
+        "CrB200SolverBindGeometrySdfData": (i, [vp, vp]),
+        "CrB200SolverGetGridDims": (i, [vp, vp]),
+        "CrB200SolverCopyParticleState": (i, [vp, u, vp, vp, vp]),
+        "CrB200SolverSetParticleState": (i, [vp, u, vp, vp, vp]),
+        "CrB200SolverCopySortState": (i, [vp, vp, vp, C.POINTER(u)]),
+        "CrB200SolverCopyCutMasks": (i, [vp, vp]),
+        "CrB200SolverGetStatus": (i, [vp, C.POINTER(u), i]),
+        "CrB200SolverClearStatus": (i, [vp]),
+        "CrB200SolverSetOption": (i, [vp, i, i]),
+        "CrB200SolverAdvance": (i, [vp, f, vp, vp, C.POINTER(i)]),
+        "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
+        "CrB200SolverGetGridStats": (i, [vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    """Every function name declared in include/crmpm_b200.h."""
+    import re
+
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"CRB200_API\s+[\w\s\*]+?\b(CrB200\w+)\s*\(", txt)))
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != OK:
+        msg = lib().CrB200GetLastError().decode()
+        raise CrmpmError(f"{what} failed ({rc}): {msg}")
+
+
+def kernel_launch_count() -> int:
+    return int(lib().CrB200GetKernelLaunchCount())
+
+
+class GpuSolver:
+    """One B200 solver behind the reference's MpmSolver interface (device pointers are ints)."""
+
+    def __init__(self, solver_type: int, num_max_particles: int, cell_size: float, grid_min, grid_max,
+                 stream: int | None = None):
+        L = lib()
+        mn = (C.c_float * 3)(*[float(v) for v in grid_min])
+        mx = (C.c_float * 3)(*[float(v) for v in grid_max])
+        h = C.c_void_p()
+        check(L.CrB200SolverCreate(int(solver_type), int(num_max_particles), C.c_float(cell_size), mn, mx,
+                                   C.c_void_p(stream or 0), C.byref(h)), "CrB200SolverCreate")
+        self._h = h
+        self._keep = []
+
+    def release(self) -> None:
+        if self._h:
+            check(lib().CrB200SolverRelease(self._h), "release")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    # -- MpmSolver -------------------------------------------------------------------------
+    def initialize(self):
+        check(lib().CrB200SolverInitialize(self._h), "initialize")
+
+    def step(self) -> float:
+        dt = C.c_float()
+        check(lib().CrB200SolverStep(self._h, C.byref(dt)), "step")
+        return dt.value
+
+    def step_many(self, n: int):
+        check(lib().CrB200SolverStepMany(self._h, int(n)), "step_many")
+
+    def fetch_results(self):
+        check(lib().CrB200SolverFetchResults(self._h), "fetch_results")
+
+    def compute_initial_data(self, n: int, indices_ptr: int):
+        check(lib().CrB200SolverComputeInitialData(self._h, int(n), C.c_void_p(indices_ptr)), "compute_initial_data")
+
+    def set_gravity(self, g):
+        check(lib().CrB200SolverSetGravity(self._h, *[C.c_float(float(v)) for v in g]), "set_gravity")
+
+    def set_integration_step_size(self, dt: float):
+        check(lib().CrB200SolverSetIntegrationStepSize(self._h, C.c_float(dt)), "set_integration_step_size")
+
+    def set_solver_iterations(self, n: int):
+        check(lib().CrB200SolverSetSolverIterations(self._h, int(n)), "set_solver_iterations")
+
+    def set_shape_contact_model(self, m: int):
+        check(lib().CrB200SolverSetShapeContactModel(self._h, int(m)), "set_shape_contact_model")
+
+    def set_num_active_particles(self, n: int):
+        check(lib().CrB200SolverSetNumActiveParticles(self._h, int(n)), "set_num_active_particles")
+
+    def bind_particle_data(self, pos_ptr: int, vel_ptr: int):
+        check(lib().CrB200SolverBindParticleData(self._h, C.c_void_p(pos_ptr), C.c_void_p(vel_ptr)), "bind_particle_data")
+
+    def bind_particle_materials(self, params_ptr: int, type_ptr: int):
+        check(lib().CrB200SolverBindParticleMaterials(self._h, C.c_void_p(params_ptr), C.c_void_p(type_ptr)),
+              "bind_particle_materials")
+
+    def bind_active_mask(self, mask_ptr: int):
+        check(lib().CrB200SolverBindActiveMask(self._h, C.c_void_p(mask_ptr)), "bind_active_mask")
+
+    def set_num_shapes(self, n: int):
+        check(lib().CrB200SolverSetNumShapes(self._h, int(n)), "set_num_shapes")
+
+    def bind_shape_ids(self, ptr: int):
+        check(lib().CrB200SolverBindShapeIds(self._h, C.c_void_p(ptr)), "bind_shape_ids")
+
+    def bind_shape_data(self, sd: ShapeDataC):
+        self._keep.append(sd)
+        check(lib().CrB200SolverBindShapeData(self._h, C.byref(sd)), "bind_shape_data")
+
+    def bind_geometry_data(self, gd: GeometryDataC):
+        self._keep.append(gd)
+        check(lib().CrB200SolverBindGeometryData(self._h, C.byref(gd)), "bind_geometry_data")
+
+    def bind_geometry_sdf_data(self, sd: GeometrySdfDataC):
+        self._keep.append(sd)
+        check(lib().CrB200SolverBindGeometrySdfData(self._h, C.byref(sd)), "bind_geometry_sdf_data")
+
+    # -- additions ---------------------------------------------------------------------------
+    def grid_dims(self):
+        out = (C.c_int * 3)()
+        check(lib().CrB200SolverGetGridDims(self._h, out), "grid_dims")
+        return tuple(out)
+
+    def copy_particle_state(self, n: int, F_ptr=0, C_ptr=0, V0_ptr=0):
+        check(lib().CrB200SolverCopyParticleState(self._h, int(n), C.c_void_p(F_ptr), C.c_void_p(C_ptr),
+                                                  C.c_void_p(V0_ptr)), "copy_particle_state")
+
+    def set_particle_state(self, n: int, F_ptr=0, C_ptr=0, V0_ptr=0):
+        check(lib().CrB200SolverSetParticleState(self._h, int(n), C.c_void_p(F_ptr), C.c_void_p(C_ptr),
+                                                 C.c_void_p(V0_ptr)), "set_particle_state")
+
+    def copy_sort_state(self, keys_ptr=0, ids_ptr=0) -> int:
+        n = C.c_uint()
+        check(lib().CrB200SolverCopySortState(self._h, C.c_void_p(keys_ptr), C.c_void_p(ids_ptr), C.byref(n)),
+              "copy_sort_state")
+        return n.value
+
+    def copy_cut_masks(self, ptr: int):
+        check(lib().CrB200SolverCopyCutMasks(self._h, C.c_void_p(ptr)), "copy_cut_masks")
+
+    def status(self, timeout_ms: int = 1000) -> int:
+        s = C.c_uint()
+        check(lib().CrB200SolverGetStatus(self._h, C.byref(s), int(timeout_ms)), "status")
+        return s.value
+
+    def clear_status(self):
+        check(lib().CrB200SolverClearStatus(self._h), "clear_status")
+
+    def set_option(self, opt: int, value: int):
+        check(lib().CrB200SolverSetOption(self._h, int(opt), int(value)), "set_option")
+
+    def advance(self, dt: float, host_pos_ptr: int = 0, host_vel_ptr: int = 0) -> int:
+        """Scene-style advance: substeps until the float time reaches dt, then read back x / v."""
+        n = C.c_int()
+        check(lib().CrB200SolverAdvance(self._h, C.c_float(dt), C.c_void_p(host_pos_ptr), C.c_void_p(host_vel_ptr),
+                                        C.byref(n)), "advance")
+        return n.value
+
+    def phase_times(self, reset: bool = True):
+        ms = (C.c_float * 4)()
+        n = C.c_int()
+        check(lib().CrB200SolverGetPhaseTimes(self._h, ms, C.byref(n), int(reset)), "phase_times")
+        return list(ms), n.value
+
+    def grid_stats(self):
+        out = (C.c_uint * 4)()
+        check(lib().CrB200SolverGetGridStats(self._h, out), "grid_stats")
+        return dict(num_sorted=out[0], active_blocks=out[1], touched_blocks=out[2], touched_nodes=out[3])
+
+
+class DeviceScene:
+    """Device buffers of one scene bound to a GpuSolver (torch is used for device memory only)."""
+
+    def __init__(self, scene, num_max: int | None = None, device: str = "cuda:0", stream=None,
+                 compute_initial: bool = True):
+        import torch
+
+        self.torch = torch
+        self.scene = scene
+        self.device = torch.device(device)
+        n = scene.n
+        self.num_max = num_max or n
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=self.device)
+        dev = self.device
+
+        def up(a, dtype=None, rows=None):
+            a = np.ascontiguousarray(a)
+            if rows is not None and a.shape[0] < rows:
+                pad = np.zeros((rows - a.shape[0],) + a.shape[1:], a.dtype)
+                a = np.concatenate([a, pad])
+            t = torch.from_numpy(a).to(dev)
+            return t
+
+        nm = self.num_max
+        self.pos = up(scene.pos_mass, rows=nm)
+        self.vel = up(scene.vel, rows=nm)
+        self.matp = up(scene.mat_params, rows=nm)
+        self.matt = up(scene.mat_type.astype(np.int32), rows=nm)
+        self.mask = up(scene.mask.astype(np.uint8), rows=nm)
+        st = scene.shapes
+        self.sh = {}
+        for k in ("shape_type", "geom_idx", "position", "rotation", "inv_scale", "lin_vel", "ang_vel", "com_inv_mass",
+                  "inertia0", "inertia1", "force", "torque", "params0", "geom_type", "geom_params", "sdf_dims",
+                  "sdf_lbcs", "sdf_data", "shape_ids"):
+            v = getattr(st, k)
+            if v.shape[0] == 0:
+                v = np.zeros((1,) + v.shape[1:], v.dtype)
+            self.sh[k] = up(v)
+        torch.cuda.synchronize(dev)
+        self.solver = GpuSolver(scene.solver_type, nm, scene.cell_size, scene.grid_min, scene.grid_max,
+                                stream=self.stream.cuda_stream)
+        s = self.solver
+        s.set_gravity(scene.gravity)
+        s.set_integration_step_size(scene.dt)
+        s.set_solver_iterations(scene.iterations)
+        s.set_shape_contact_model(scene.contact_model)
+        s.bind_particle_data(self.pos.data_ptr(), self.vel.data_ptr())
+        s.bind_particle_materials(self.matp.data_ptr(), self.matt.data_ptr())
+        s.bind_active_mask(self.mask.data_ptr())
+        s.set_num_active_particles(n)
+        p = {k: v.data_ptr() for k, v in self.sh.items()}
+        s.bind_shape_data(ShapeDataC(p["shape_type"], p["geom_idx"], p["position"], p["rotation"], p["inv_scale"],
+                                     p["lin_vel"], p["ang_vel"], p["com_inv_mass"], p["inertia0"], p["inertia1"],
+                                     p["force"], p["torque"], p["params0"], int(st.shape_type.shape[0])))
+        s.bind_geometry_data(GeometryDataC(p["geom_type"], p["geom_params"], int(st.geom_type.shape[0])))
+        s.bind_geometry_sdf_data(GeometrySdfDataC(p["sdf_dims"], p["sdf_lbcs"], p["sdf_data"]))
+        s.bind_shape_ids(p["shape_ids"])
+        s.set_num_shapes(st.num_shapes)
+        s.initialize()
+        if compute_initial:
+            self.compute_initial_data()
+
+    def compute_initial_data(self, idx=None):
+        torch = self.torch
+        idx = np.arange(self.scene.n, dtype=np.uint32) if idx is None else np.asarray(idx, np.uint32)
+        self._idx = torch.from_numpy(idx.astype(np.int32)).to(self.device)
+        torch.cuda.synchronize(self.device)
+        self.solver.compute_initial_data(idx.shape[0], self._idx.data_ptr())
+
+    def step(self, k: int = 1, graph: bool = True):
+        if graph and k > 1:
+            self.solver.step_many(k)
+        else:
+            for _ in range(k):
+                self.solver.step()
+
+    def sync(self):
+        self.solver.fetch_results()
+
+    def set_shape(self, shape_id: int, position=None, lin_vel=None, rotation=None, ang_vel=None):
+        """Update one shape's pose / velocity on the solver stream (what a factory sync does)."""
+        torch = self.torch
+        with torch.cuda.stream(self.stream):
+            for key, val in (("position", position), ("lin_vel", lin_vel), ("rotation", rotation), ("ang_vel", ang_vel)):
+                if val is not None:
+                    v = list(val) + [0.0] * (4 - len(val))
+                    self.sh[key][shape_id] = torch.tensor(v[:4], dtype=torch.float32, device=self.device)
+
+    def state(self):
+        torch = self.torch
+        n = self.scene.n
+        F = torch.empty((n, 9), dtype=torch.float32, device=self.device)
+        Cm = torch.empty((n, 9), dtype=torch.float32, device=self.device)
+        V0 = torch.empty(n, dtype=torch.float32, device=self.device)
+        self.solver.copy_particle_state(n, F.data_ptr(), Cm.data_ptr(), V0.data_ptr())
+        self.sync()
+        return dict(x=self.pos[:n, :3].cpu().numpy(), m=self.pos[:n, 3].cpu().numpy(), v=self.vel[:n, :3].cpu().numpy(),
+                    F=F.cpu().numpy(), C=Cm.cpu().numpy(), V0=V0.cpu().numpy())
+
+    def set_state(self, F=None, Cm=None, V0=None):
+        torch = self.torch
+        n = self.scene.n
+        ts = [None if a is None else torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(self.device)
+              for a in (F, Cm, V0)]
+        torch.cuda.synchronize(self.device)
+        self.solver.set_particle_state(n, *[0 if t is None else t.data_ptr() for t in ts])
+        self.sync()
+
+    def sort_state(self):
+        torch = self.torch
+        n = self.scene.n
+        keys = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        ids = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        cnt = self.solver.copy_sort_state(keys.data_ptr(), ids.data_ptr())
+        self.sync()
+        return keys[:n].cpu().numpy().view(np.uint32), ids[:cnt].cpu().numpy().view(np.uint32)
+
+    def cut_masks(self):
+        torch = self.torch
+        n = self.scene.n
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+        self.solver.copy_cut_masks(out.data_ptr())
+        self.sync()
+        return out[:n].cpu().numpy().view(np.uint32)
+
+    def coupling(self):
+        self.sync()
+        return self.sh["force"].cpu().numpy(), self.sh["torque"].cpu().numpy()

@@ -1,0 +1,782 @@
+// Device-side math, SDF geometry, rigid contact and slicer predicates of the B200 MPM engine.
+//
+// The formulas restate CRESSim-MPM's L1 functions (paths are inside the reference project):
+//   quaternion rotation          include/math/quat.h:117-150
+//   analytic / grid SDFs         include/geometry_utils/sdf.h:67-662
+//   rigid contact and friction   src/solver/mpm_rigid_contact.h:101-399
+//   slicer side test (cutting)   src/solver/mpm_rigid_contact.h:401-478
+// Everything that feeds an integer or boolean result compared bit for bit (cell keys, slicer
+// masks) is evaluated with explicitly rounded operations (__fmul_rn / __fadd_rn / ...), i.e. with
+// no fused multiply-add, so that it equals the reference's host arithmetic on identical inputs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace crb200
+{
+    constexpr float kEps = 1.1920928955078125e-07f; // FLT_EPSILON, the reference's CR_EPS
+    constexpr float kMaxF32 = 3.4028234663852885981170418348452e+38F;
+    constexpr int kMaxShapes = 64;
+
+    enum GeomType : int
+    {
+        G_BOX = 0, G_SPHERE, G_PLANE, G_CAPSULE, G_TRIMESH, G_QUAD_SLICER, G_TRIMESH_SLICER, G_LINES, G_ARC
+    };
+    enum ShapeKind : int { S_STATIC = 0, S_KINEMATIC = 1, S_DYNAMIC = 2 };
+
+    enum ShapeFlags : int
+    {
+        SF_SLICER = 1,  // at least one slicer geometry: P2G/G2P must test node sides
+        SF_DYNAMIC = 2, // at least one dynamic shape: grid contact accumulates coupling force
+    };
+
+    // One rigid shape of a scene, gathered once per substep from the bound struct-of-arrays.
+    struct __align__(16) ShapeRec
+    {
+        float4 pos, rot, invScale, linVel, angVel, params0, gparams, comInvMass, inertia0, inertia1;
+        int kind, gtype, id, pad;
+    };
+
+    struct SdfPtrs
+    {
+        const int4 *dim;
+        const float4 *lbcs;
+        const float4 *data;
+    };
+
+    // ---------------------------------------------------------------------------------------
+    // small vector helpers (fused multiply-add allowed)
+    struct V3
+    {
+        float x, y, z;
+    };
+    __device__ __forceinline__ V3 v3(float a, float b, float c) { return V3{a, b, c}; }
+    __device__ __forceinline__ V3 v3(const float4 &f) { return V3{f.x, f.y, f.z}; }
+    __device__ __forceinline__ V3 v3(const float3 &f) { return V3{f.x, f.y, f.z}; }
+    __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+    __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+    __device__ __forceinline__ V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+    __device__ __forceinline__ V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
+    __device__ __forceinline__ V3 mul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+    __device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+    __device__ __forceinline__ V3 cross(V3 a, V3 b)
+    {
+        return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    }
+    __device__ __forceinline__ float sq(V3 a) { return dot(a, a); }
+    __device__ __forceinline__ V3 normalized(V3 v)
+    {
+        float s = sq(v);
+        return s > 0.f ? v * rsqrtf(s) : v;
+    }
+    __device__ __forceinline__ float comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+    // Quaternion rotation (quat.h:117-150).
+    __device__ __forceinline__ V3 qrot(const float4 &q, V3 v)
+    {
+        const float vx = 2.f * v.x, vy = 2.f * v.y, vz = 2.f * v.z;
+        const float w2 = q.w * q.w - 0.5f;
+        const float d2 = q.x * vx + q.y * vy + q.z * vz;
+        return v3(vx * w2 + (q.y * vz - q.z * vy) * q.w + q.x * d2, vy * w2 + (q.z * vx - q.x * vz) * q.w + q.y * d2,
+                  vz * w2 + (q.x * vy - q.y * vx) * q.w + q.z * d2);
+    }
+    __device__ __forceinline__ V3 qrotInv(const float4 &q, V3 v)
+    {
+        const float vx = 2.f * v.x, vy = 2.f * v.y, vz = 2.f * v.z;
+        const float w2 = q.w * q.w - 0.5f;
+        const float d2 = q.x * vx + q.y * vy + q.z * vz;
+        return v3(vx * w2 - (q.y * vz - q.z * vy) * q.w + q.x * d2, vy * w2 - (q.z * vx - q.x * vz) * q.w + q.y * d2,
+                  vz * w2 - (q.x * vy - q.y * vx) * q.w + q.z * d2);
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Exactly rounded arithmetic (no contraction) for bit-exact integer and side outputs.
+    namespace ex
+    {
+        __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+        __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+        __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+        __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+        __device__ __forceinline__ V3 add(V3 a, V3 b) { return v3(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)); }
+        __device__ __forceinline__ V3 sub(V3 a, V3 b) { return v3(sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)); }
+        __device__ __forceinline__ V3 mul(V3 a, V3 b) { return v3(mul(a.x, b.x), mul(a.y, b.y), mul(a.z, b.z)); }
+        __device__ __forceinline__ V3 muls(V3 a, float s) { return v3(mul(a.x, s), mul(a.y, s), mul(a.z, s)); }
+        __device__ __forceinline__ float dot(V3 a, V3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+
+        // quat.h:137-150, evaluated left to right as the host compiles it.
+        __device__ __forceinline__ V3 qrotInv(const float4 &q, V3 v)
+        {
+            const float vx = mul(2.f, v.x), vy = mul(2.f, v.y), vz = mul(2.f, v.z);
+            const float w2 = sub(mul(q.w, q.w), 0.5f);
+            const float d2 = add(add(mul(q.x, vx), mul(q.y, vy)), mul(q.z, vz));
+            return v3(add(sub(mul(vx, w2), mul(sub(mul(q.y, vz), mul(q.z, vy)), q.w)), mul(q.x, d2)),
+                      add(sub(mul(vy, w2), mul(sub(mul(q.z, vx), mul(q.x, vz)), q.w)), mul(q.y, d2)),
+                      add(sub(mul(vz, w2), mul(sub(mul(q.x, vy), mul(q.y, vx)), q.w)), mul(q.z, d2)));
+        }
+
+        // Trilinear SDF distance with the reference's value/weight pairing (sdf.h:243-276).
+        __device__ __forceinline__ float trilinear(const SdfPtrs &s, int4 dim, int off, int bx, int by, int bz, V3 fr)
+        {
+            float vals[8];
+#pragma unroll
+            for (int dx = 0; dx <= 1; ++dx)
+#pragma unroll
+                for (int dy = 0; dy <= 1; ++dy)
+#pragma unroll
+                    for (int dz = 0; dz <= 1; ++dz)
+                        vals[(dx << 2) | (dy << 1) | dz] =
+                            __ldg(&s.data[off + ((bz + dz) * dim.x * dim.y) + ((by + dy) * dim.x) + (bx + dx)].w);
+            const float ox = sub(1.f, fr.x), oy = sub(1.f, fr.y), oz = sub(1.f, fr.z);
+            const float w[8] = {mul(mul(ox, oy), oz), mul(mul(fr.x, oy), oz), mul(mul(ox, fr.y), oz),
+                                mul(mul(fr.x, fr.y), oz), mul(mul(ox, oy), fr.z), mul(mul(fr.x, oy), fr.z),
+                                mul(mul(ox, fr.y), fr.z), mul(mul(fr.x, fr.y), fr.z)};
+            float acc = 0.f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                acc = add(acc, mul(vals[i], w[i]));
+            return acc;
+        }
+
+        // getGeometryModSdf (sdf.h:504-662): does the point project onto the slicer surface, and
+        // on which side (signed distance in *d, gradient in *g).
+        __device__ __forceinline__ bool modSdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, float *d, V3 *g)
+        {
+            if (gtype == G_QUAD_SLICER)
+            {
+                if (lp.x < -p0.x || lp.x > p0.x || lp.z < -p0.y || lp.z > p0.y)
+                    return false;
+                *g = v3(0.f, copysignf(1.f, lp.y), 0.f);
+                *d = lp.y;
+                return true;
+            }
+            if (gtype == G_TRIMESH_SLICER)
+            {
+                int off = __float_as_int(p0.x);
+                const float4 spine = __ldg(&s.data[off]);
+                if (isnan(spine.x))
+                    return false;
+                if (add(ex::dot(lp, v3(spine)), spine.w) > 0.f)
+                    return false;
+                off++;
+                const int id = __float_as_int(p0.y);
+                const float4 lb = __ldg(&s.lbcs[id]);
+                const int4 dim = __ldg(&s.dim[id]);
+                const V3 sp = v3(div(sub(lp.x, lb.x), lb.w), div(sub(lp.y, lb.y), lb.w), div(sub(lp.z, lb.z), lb.w));
+                const int qx = __float2int_rz(add(sp.x, 0.5f)), qy = __float2int_rz(add(sp.y, 0.5f)),
+                          qz = __float2int_rz(add(sp.z, 0.5f));
+                if (qx < 1 || qx >= dim.x - 1 || qy < 1 || qy >= dim.y - 1 || qz < 1 || qz >= dim.z - 1)
+                    return false;
+                const float4 qv = __ldg(&s.data[off + (qz * dim.x * dim.y) + (qy * dim.x) + qx]);
+                if (isnan(qv.w))
+                    return false;
+                const int bx = __float2int_rz(sp.x), by = __float2int_rz(sp.y), bz = __float2int_rz(sp.z);
+                const V3 fr = v3(sub(sp.x, (float)bx), sub(sp.y, (float)by), sub(sp.z, (float)bz));
+                const float iv = trilinear(s, dim, off, bx, by, bz, fr);
+                if (isnan(iv))
+                    return false;
+                *d = iv;
+                *g = (mul(qv.w, iv) < 0.f) ? v3(-qv.x, -qv.y, -qv.z) : v3(qv);
+                return true;
+            }
+            return false;
+        }
+    } // namespace ex
+
+    // checkOnDifferentSides (mpm_rigid_contact.h:401-478) for particle p1 and node position p2,
+    // both given exactly as the reference forms them.  *normal (optional) is the side gradient at
+    // p2 in the shape's local frame, as the reference returns it.
+    __device__ __forceinline__ bool differentSides(V3 p1, V3 p2, const ShapeRec *sh, int num, const SdfPtrs &sdf,
+                                                   V3 *normal)
+    {
+        for (int s = 0; s < num; ++s)
+        {
+            const ShapeRec &r = sh[s];
+            if (r.gtype != G_QUAD_SLICER && r.gtype != G_TRIMESH_SLICER)
+                continue;
+            const V3 pos = v3(r.pos), isc = v3(r.invScale);
+            const V3 r1 = ex::mul(ex::qrotInv(r.rot, ex::sub(p1, pos)), isc);
+            float d1, d2;
+            V3 g1, g2;
+            if (!ex::modSdf(r1, r.gtype, r.gparams, sdf, &d1, &g1))
+                continue;
+            const V3 r2 = ex::mul(ex::qrotInv(r.rot, ex::sub(p2, pos)), isc);
+            if (ex::modSdf(r2, r.gtype, r.gparams, sdf, &d2, &g2) && (signbit(d1) != signbit(d2)))
+            {
+                if (normal)
+                {
+                    V3 g = mul(g2, isc);
+                    *normal = g * rsqrtf(sq(g));
+                }
+                return true;
+            }
+        }
+        return false;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // getGeometrySdf (sdf.h:67-496): gradient/distance in the shape's local (unscaled) frame.
+    // Returns the slicer-spine flag; *tangent is written for lines and arcs.
+    __device__ __forceinline__ float trilinearF(const SdfPtrs &s, int4 dim, int off, int bx, int by, int bz, V3 fr)
+    {
+        float vals[8];
+#pragma unroll
+        for (int dx = 0; dx <= 1; ++dx)
+#pragma unroll
+            for (int dy = 0; dy <= 1; ++dy)
+#pragma unroll
+                for (int dz = 0; dz <= 1; ++dz)
+                    vals[(dx << 2) | (dy << 1) | dz] =
+                        __ldg(&s.data[off + ((bz + dz) * dim.x * dim.y) + ((by + dy) * dim.x) + (bx + dx)].w);
+        const float ox = 1.f - fr.x, oy = 1.f - fr.y, oz = 1.f - fr.z;
+        const float w[8] = {ox * oy * oz, fr.x * oy * oz, ox * fr.y * oz, fr.x * fr.y * oz,
+                            ox * oy * fr.z, fr.x * oy * fr.z, ox * fr.y * fr.z, fr.x * fr.y * fr.z};
+        float acc = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            acc += vals[i] * w[i];
+        return acc;
+    }
+
+    static __device__ __noinline__ bool geometrySdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, V3 &grad, float &dist,
+                                             V3 &tangent)
+    {
+        bool inSpine = false;
+        switch (gtype)
+        {
+        case G_BOX:
+        {
+            const V3 pen = v3(fabsf(lp.x) - p0.x, fabsf(lp.y) - p0.y, fabsf(lp.z) - p0.z);
+            const V3 sg = v3(lp.x < 0.f ? -1.f : 1.f, lp.y < 0.f ? -1.f : 1.f, lp.z < 0.f ? -1.f : 1.f);
+            const float g = fmaxf(pen.x, fmaxf(pen.y, pen.z));
+            const V3 q = v3(fmaxf(pen.x, 0.f), fmaxf(pen.y, 0.f), fmaxf(pen.z, 0.f));
+            const float l = sqrtf(sq(q));
+            V3 dir;
+            if (g > 0.f)
+                dir = q / l;
+            else if (pen.x > pen.y)
+                dir = (pen.x > pen.z) ? v3(1.f, 0.f, 0.f) : v3(0.f, 0.f, 1.f);
+            else
+                dir = (pen.y > pen.z) ? v3(0.f, 1.f, 0.f) : v3(0.f, 0.f, 1.f);
+            grad = mul(sg, dir);
+            dist = l + fminf(g, 0.f);
+            break;
+        }
+        case G_SPHERE:
+        {
+            const float len = sqrtf(sq(lp));
+            grad = lp / fmaxf(len, kEps);
+            dist = len - p0.x;
+            break;
+        }
+        case G_PLANE:
+            grad = v3(0.f, 1.f, 0.f);
+            dist = lp.y;
+            break;
+        case G_CAPSULE:
+        {
+            const float h2 = p0.y * 2.f;
+            V3 pa = lp;
+            pa.y -= p0.y;
+            const float h = fminf(fmaxf(-pa.y / h2, 0.f), 1.f);
+            pa.y += h2 * h;
+            const float d = sqrtf(sq(pa));
+            grad = pa / fmaxf(d, kEps);
+            dist = d - p0.x;
+            break;
+        }
+        case G_ARC:
+        {
+            const float ang = atan2f(lp.z, lp.x);
+            if (ang < p0.x || ang > p0.y)
+            {
+                grad = v3(0.f, 1.f, 0.f);
+                dist = __int_as_float(0x7fc00000);
+                break;
+            }
+            float sn, cs;
+            sincosf(ang, &sn, &cs);
+            const V3 ptp = lp - v3(cs, 0.f, sn);
+            const float d = sqrtf(sq(ptp));
+            grad = ptp / fmaxf(d, kEps);
+            dist = d;
+            tangent = v3(-sn, 0.f, cs);
+            break;
+        }
+        case G_TRIMESH:
+        {
+            const int off = __float_as_int(p0.x), id = __float_as_int(p0.y);
+            const float4 lb = __ldg(&s.lbcs[id]);
+            const int4 dim = __ldg(&s.dim[id]);
+            const V3 sp = (lp - v3(lb)) / lb.w;
+            const int qx = __float2int_rz(sp.x + 0.5f), qy = __float2int_rz(sp.y + 0.5f), qz = __float2int_rz(sp.z + 0.5f);
+            if (qx < 0 || qx >= dim.x || qy < 0 || qy >= dim.y || qz < 0 || qz >= dim.z)
+            {
+                grad = v3(0.f, 1.f, 0.f);
+                dist = kMaxF32;
+                break;
+            }
+            const float4 qv = __ldg(&s.data[off + (qz * dim.x * dim.y) + (qy * dim.x) + qx]);
+            grad = v3(qv);
+            const int bx = __float2int_rz(sp.x), by = __float2int_rz(sp.y), bz = __float2int_rz(sp.z);
+            if (bx < 0 || bx >= dim.x - 1 || by < 0 || by >= dim.y - 1 || bz < 0 || bz >= dim.z - 1)
+            {
+                dist = qv.w;
+                break;
+            }
+            dist = trilinearF(s, dim, off, bx, by, bz, v3(sp.x - (float)bx, sp.y - (float)by, sp.z - (float)bz));
+            break;
+        }
+        case G_QUAD_SLICER:
+        {
+            if (lp.x < -p0.x || lp.x > p0.x || lp.z < -p0.y || lp.z > p0.y)
+            {
+                grad = v3(0.f, 0.f, 0.f);
+                dist = kMaxF32;
+            }
+            else
+            {
+                grad = v3(0.f, copysignf(1.f, lp.y), 0.f);
+                dist = fabsf(lp.y);
+            }
+            break;
+        }
+        case G_TRIMESH_SLICER:
+        {
+            grad = v3(0.f, 1.f, 0.f);
+            dist = __int_as_float(0x7fc00000);
+            const int off = __float_as_int(p0.x) + 1, id = __float_as_int(p0.y);
+            const float4 lb = __ldg(&s.lbcs[id]);
+            const int4 dim = __ldg(&s.dim[id]);
+            const V3 sp = (lp - v3(lb)) / lb.w;
+            const int qx = __float2int_rz(sp.x + 0.5f), qy = __float2int_rz(sp.y + 0.5f), qz = __float2int_rz(sp.z + 0.5f);
+            if (qx < 1 || qx >= dim.x - 1 || qy < 1 || qy >= dim.y - 1 || qz < 1 || qz >= dim.z - 1)
+                break;
+            const float4 qv = __ldg(&s.data[off + (qz * dim.x * dim.y) + (qy * dim.x) + qx]);
+            if (isnan(qv.w))
+                break;
+            grad = v3(qv);
+            const int bx = __float2int_rz(sp.x), by = __float2int_rz(sp.y), bz = __float2int_rz(sp.z);
+            const float iv = trilinearF(s, dim, off, bx, by, bz, v3(sp.x - (float)bx, sp.y - (float)by, sp.z - (float)bz));
+            if (isnan(iv))
+                break;
+            dist = fabsf(iv);
+            if (qv.w * iv < 0.f)
+                grad = v3(-grad.x, -grad.y, -grad.z);
+            const float4 spine = __ldg(&s.data[off - 1]);
+            if (isnan(spine.x))
+                break;
+            const V3 sn = v3(spine);
+            const float len = sqrtf(sq(sn));
+            if (dot(lp, sn / len) + spine.w > 0.f)
+            {
+                dist -= len - 1.f;
+                inSpine = true;
+            }
+            break;
+        }
+        case G_LINES:
+        {
+            grad = v3(0.f, 1.f, 0.f);
+            dist = __int_as_float(0x7fc00000);
+            const int off = __float_as_int(p0.x), id = __float_as_int(p0.y), size = __float_as_int(p0.z);
+            const float4 bmin = __ldg(&s.lbcs[id]), bmax = __ldg(&s.data[off]);
+            if (lp.x < bmin.x || lp.x > bmax.x || lp.y < bmin.y || lp.y > bmax.y || lp.z < bmin.z || lp.z > bmax.z)
+                break;
+            int closestIdx = 0;
+            V3 closest = v3(0.f, 0.f, 0.f), pt1 = v3(0.f, 0.f, 0.f);
+            float closestD = kMaxF32;
+            for (int p = off + 1; p < off + size - 1; ++p)
+            {
+                const V3 a = v3(__ldg(&s.data[p]));
+                pt1 = v3(__ldg(&s.data[p + 1]));
+                const V3 line = pt1 - a;
+                float t = dot(lp - a, line) / sq(line);
+                t = fmaxf(0.f, fminf(1.f, t));
+                const V3 proj = a + line * t;
+                const float d = sqrtf(sq(lp - proj));
+                if (d < closestD)
+                {
+                    closestD = d;
+                    closest = proj;
+                    closestIdx = p;
+                }
+            }
+            const V3 pt0 = v3(__ldg(&s.data[off + 1]));
+            if (sq(closest - pt0) < kEps || sq(closest - pt1) < kEps)
+                break;
+            grad = normalized(lp - closest);
+            tangent = normalized(v3(__ldg(&s.data[closestIdx])) - v3(__ldg(&s.data[closestIdx + 1])));
+            dist = closestD;
+            break;
+        }
+        default:
+            break;
+        }
+        return inSpine;
+    }
+
+    // resolveRigidCollision (mpm_rigid_contact.h:101-399).
+    //   isParticle = false: grid node with velocity vel (mass m) evaluated at pos; contact inside
+    //       the smooth distance, separating nodes skipped, Coulomb-like friction, drag, rigid
+    //       velocity, line/arc tangent restriction, dynamic coupling (kinematic or effective mass).
+    //   isParticle = true: positional push-out only (lines and arcs skipped).
+    template <bool IsParticle>
+    __device__ __forceinline__ void rigidContact(V3 &vel, float m, V3 &pos, const ShapeRec *sh, int num, const SdfPtrs &sdf,
+                                                 bool effMass, float4 *coupleForce, float4 *coupleTorque)
+    {
+        for (int s = 0; s < num; ++s)
+        {
+            const ShapeRec &r = sh[s];
+            if (IsParticle && (r.gtype == G_LINES || r.gtype == G_ARC))
+                continue;
+            const V3 isc = v3(r.invScale);
+            const V3 wrel = pos - v3(r.pos);
+            const V3 lp = mul(qrotInv(r.rot, wrel), isc);
+            V3 grad, tangent = v3(0.f, 0.f, 0.f);
+            float dist;
+            const bool onSpine = geometrySdf(lp, r.gtype, r.gparams, sdf, grad, dist, tangent);
+            if (isnan(dist))
+                continue;
+            grad = mul(grad, isc);
+            const float is = rsqrtf(sq(grad));
+            dist = dist * is - r.params0.w;
+            grad = grad * is;
+            const float smooth = IsParticle ? 0.f : r.params0.x;
+            if (!(dist < smooth))
+                continue;
+            const V3 normal = qrot(r.rot, grad);
+            const V3 rigidVel = r.kind == S_STATIC ? v3(0.f, 0.f, 0.f) : v3(r.linVel) + cross(v3(r.angVel), wrel);
+            const V3 relVel = vel - rigidVel;
+            const float vn = dot(relVel, normal);
+            if (IsParticle)
+            {
+                pos = pos - normal * fminf(dist, 0.f);
+                continue;
+            }
+            if (vn >= 0.f)
+                continue;
+            const float friction = onSpine ? 100.f : r.params0.z;
+            const float sticky = r.params0.y;
+            V3 resp;
+            if (effMass && r.kind == S_DYNAMIC)
+            {
+                resp = v3(0.f, 0.f, 0.f); // zero unless the impulse below is defined (:231)
+                const float invMassRigid = r.comInvMass.w;
+                if (invMassRigid > 0.f)
+                {
+                    const V3 rr = wrel - qrot(r.rot, v3(r.comInvMass));
+                    const V3 rxnl = qrotInv(r.rot, cross(rr, normal));
+                    const V3 wl = v3(r.inertia0.x * rxnl.x + r.inertia1.x * rxnl.y + r.inertia1.y * rxnl.z,
+                                     r.inertia1.x * rxnl.x + r.inertia0.y * rxnl.y + r.inertia1.z * rxnl.z,
+                                     r.inertia1.y * rxnl.x + r.inertia1.z * rxnl.y + r.inertia0.z * rxnl.z);
+                    const V3 tt = cross(qrot(r.rot, wl), rr);
+                    const float invMassGrid = 1.f / m;
+                    const float invMassComb = invMassGrid + (invMassRigid + dot(normal, tt));
+                    if (invMassComb > 0.f)
+                    {
+                        const float Jn = -1.f * vn / invMassComb;
+                        const V3 vt = relVel - normal * vn;
+                        const float vtn = sqrtf(sq(vt));
+                        V3 impT = v3(0.f, 0.f, 0.f);
+                        if (vtn > kEps)
+                        {
+                            const float fJt = fminf(friction * Jn, vtn / invMassComb);
+                            const float fin = (vtn - fJt * invMassComb) * sticky;
+                            impT = (vt * -1.f / vtn) * ((vtn - fin) / invMassComb);
+                        }
+                        const V3 tot = normal * Jn + impT;
+                        resp = vel + tot * invMassGrid;
+                        const V3 mom = tot * -1.f;
+                        const V3 tq = cross(rr, mom);
+                        atomicAdd(&coupleForce[r.id].x, mom.x);
+                        atomicAdd(&coupleForce[r.id].y, mom.y);
+                        atomicAdd(&coupleForce[r.id].z, mom.z);
+                        atomicAdd(&coupleTorque[r.id].x, tq.x);
+                        atomicAdd(&coupleTorque[r.id].y, tq.y);
+                        atomicAdd(&coupleTorque[r.id].z, tq.z);
+                    }
+                }
+            }
+            else
+            {
+                V3 tang = relVel - normal * vn;
+                if (r.gtype == G_LINES || r.gtype == G_ARC)
+                {
+                    const V3 td = qrot(r.rot, normalized(mul(tangent, isc)));
+                    tang = td * dot(tang, td);
+                }
+                const float tn = sqrtf(sq(tang));
+                const float fc = fmaxf(friction * vn / (tn + kEps), -1.f);
+                resp = (tang + tang * fc) * sticky + rigidVel;
+                if (!effMass && r.kind == S_DYNAMIC)
+                {
+                    const V3 mom = (vel - resp) * m;
+                    const V3 tq = cross(pos - v3(r.pos), mom);
+                    atomicAdd(&coupleForce[r.id].x, mom.x);
+                    atomicAdd(&coupleForce[r.id].y, mom.y);
+                    atomicAdd(&coupleForce[r.id].z, mom.z);
+                    atomicAdd(&coupleTorque[r.id].x, tq.x);
+                    atomicAdd(&coupleTorque[r.id].y, tq.y);
+                    atomicAdd(&coupleTorque[r.id].z, tq.z);
+                }
+            }
+            vel = resp;
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // 3x3 matrices, column-major in registers: m[c*3 + r].
+    struct M3
+    {
+        float m[9];
+    };
+    __device__ __forceinline__ float det3(const M3 &a)
+    {
+        const float A = a.m[0], B = a.m[3], Cc = a.m[6], D = a.m[1], E = a.m[4], F = a.m[7], G = a.m[2], H = a.m[5],
+                    I = a.m[8];
+        return A * (E * I - F * H) - B * (D * I - F * G) + Cc * (D * H - E * G);
+    }
+    __device__ __forceinline__ M3 matmul(const M3 &a, const M3 &b)
+    {
+        M3 r;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr)
+                r.m[c * 3 + rr] = a.m[rr] * b.m[c * 3] + a.m[3 + rr] * b.m[c * 3 + 1] + a.m[6 + rr] * b.m[c * 3 + 2];
+        return r;
+    }
+    __device__ __forceinline__ M3 transpose(const M3 &a)
+    {
+        M3 r;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr)
+                r.m[c * 3 + rr] = a.m[rr * 3 + c];
+        return r;
+    }
+    // inverse with the reference's singular cutoff (mat33.h:256-283)
+    __device__ __forceinline__ M3 inverse3(const M3 &a)
+    {
+        const float A = a.m[0], B = a.m[3], Cc = a.m[6], D = a.m[1], E = a.m[4], F = a.m[7], G = a.m[2], H = a.m[5],
+                    I = a.m[8];
+        const float dt = A * (E * I - F * H) - B * (D * I - F * G) + Cc * (D * H - E * G);
+        M3 r;
+        if (fabsf(dt) < 1e-6f)
+        {
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                r.m[i] = 0.f;
+            return r;
+        }
+        const float inv = 1.f / dt;
+        r.m[0] = (E * I - F * H) * inv;
+        r.m[1] = -(B * I - Cc * H) * inv;
+        r.m[2] = (B * F - Cc * E) * inv;
+        r.m[3] = -(D * I - F * G) * inv;
+        r.m[4] = (A * I - Cc * G) * inv;
+        r.m[5] = -(A * F - Cc * D) * inv;
+        r.m[6] = (D * H - E * G) * inv;
+        r.m[7] = -(A * H - B * G) * inv;
+        r.m[8] = (A * E - B * D) * inv;
+        return r;
+    }
+
+    // Kirchhoff stress (constitutive_models.h:49-118).  eCoRotational falls through to the
+    // linear (St. Venant-Kirchhoff) model in the reference, so it is computed as such here.
+    __device__ __forceinline__ M3 kirchhoffStress(const M3 &F, float lambda, float mu, int type)
+    {
+        M3 s;
+        if (type == 1) // Neo-Hookean
+        {
+            float J = det3(F);
+            J = J < 1e-6f ? 1e-6f : J;
+            const float l = lambda * logf(J);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                {
+                    const float b = F.m[r] * F.m[c] + F.m[3 + r] * F.m[3 + c] + F.m[6 + r] * F.m[6 + c];
+                    s.m[c * 3 + r] = mu * (b - (r == c ? 1.f : 0.f)) + (r == c ? l : 0.f);
+                }
+        }
+        else if (type == 0 || type == 2) // co-rotational (falls through) and linear
+        {
+            M3 E;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                {
+                    const float ftf = F.m[r * 3] * F.m[c * 3] + F.m[r * 3 + 1] * F.m[c * 3 + 1] + F.m[r * 3 + 2] * F.m[c * 3 + 2];
+                    E.m[c * 3 + r] = 0.5f * (ftf - (r == c ? 1.f : 0.f));
+                }
+            const float tr = E.m[0] + E.m[4] + E.m[8];
+            M3 S;
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                S.m[i] = 2.f * mu * E.m[i];
+            S.m[0] += tr * lambda;
+            S.m[4] += tr * lambda;
+            S.m[8] += tr * lambda;
+            s = matmul(matmul(F, S), transpose(F));
+        }
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                s.m[i] = 0.f;
+        }
+        return s;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Polar rotation via SVD: A = U diag(s) V^T with U, V proper rotations and sign(det A) on s[2]
+    // (the convention of the reference's svd3: McAdams et al., UW-Madison TR1690, 2011).
+    // Jacobi eigen-analysis of A^T A with exact rotations, column sort of B = A V, Givens QR of B.
+    template <typename T>
+    __device__ __forceinline__ void svdRotations(const T A[9], T U[9], T V[9], T s[3], int sweeps)
+    {
+        T S[6]; // symmetric A^T A: s00 s11 s22 s01 s02 s12
+        auto a = [&](int r, int c) { return A[c * 3 + r]; };
+        S[0] = a(0, 0) * a(0, 0) + a(1, 0) * a(1, 0) + a(2, 0) * a(2, 0);
+        S[1] = a(0, 1) * a(0, 1) + a(1, 1) * a(1, 1) + a(2, 1) * a(2, 1);
+        S[2] = a(0, 2) * a(0, 2) + a(1, 2) * a(1, 2) + a(2, 2) * a(2, 2);
+        S[3] = a(0, 0) * a(0, 1) + a(1, 0) * a(1, 1) + a(2, 0) * a(2, 1);
+        S[4] = a(0, 0) * a(0, 2) + a(1, 0) * a(1, 2) + a(2, 0) * a(2, 2);
+        S[5] = a(0, 1) * a(0, 2) + a(1, 1) * a(1, 2) + a(2, 1) * a(2, 2);
+        T Vm[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        for (int sw = 0; sw < sweeps; ++sw)
+        {
+#pragma unroll
+            for (int pq = 0; pq < 3; ++pq)
+            {
+                const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
+                const int ipq = pq == 0 ? 3 : (pq == 1 ? 4 : 5);
+                const T apq = S[ipq];
+                if (apq == T(0))
+                    continue;
+                const T app = S[p], aqq = S[q];
+                const T theta = (aqq - app) / (T(2) * apq);
+                const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+                const T c = T(1) / sqrt(t * t + T(1)), sn = t * c;
+                // rotate S in the (p, q) plane: new diagonal and the off-diagonals with the third index
+                const int o = 3 - p - q;
+                const int ipo = (p == 0 && o == 1) || (p == 1 && o == 0) ? 3 : ((p == 0 && o == 2) || (p == 2 && o == 0) ? 4 : 5);
+                const int iqo = (q == 0 && o == 1) || (q == 1 && o == 0) ? 3 : ((q == 0 && o == 2) || (q == 2 && o == 0) ? 4 : 5);
+                const T spo = S[ipo], sqo = S[iqo];
+                S[p] = app - t * apq;
+                S[q] = aqq + t * apq;
+                S[ipq] = T(0);
+                S[ipo] = c * spo - sn * sqo;
+                S[iqo] = sn * spo + c * sqo;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    const T vkp = Vm[k][p], vkq = Vm[k][q];
+                    Vm[k][p] = c * vkp - sn * vkq;
+                    Vm[k][q] = sn * vkp + c * vkq;
+                }
+            }
+        }
+        T B[3][3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                B[r][c] = a(r, 0) * Vm[0][c] + a(r, 1) * Vm[1][c] + a(r, 2) * Vm[2][c];
+        auto n2 = [&](int c) { return B[0][c] * B[0][c] + B[1][c] * B[1][c] + B[2][c] * B[2][c]; };
+        auto swapc = [&](int x, int y) {
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                T tb = B[r][x];
+                B[r][x] = B[r][y];
+                B[r][y] = -tb;
+                T tv = Vm[r][x];
+                Vm[r][x] = Vm[r][y];
+                Vm[r][y] = -tv;
+            }
+        };
+        T c0 = n2(0), c1 = n2(1), c2 = n2(2);
+        if (c0 < c1) { swapc(0, 1); T t = c0; c0 = c1; c1 = t; }
+        if (c0 < c2) { swapc(0, 2); T t = c0; c0 = c2; c2 = t; }
+        if (c1 < c2) { swapc(1, 2); }
+        T Um[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+#pragma unroll
+        for (int gi = 0; gi < 3; ++gi)
+        {
+            const int p = gi == 2 ? 1 : 0, q = gi == 0 ? 1 : 2, col = gi == 2 ? 1 : 0;
+            const T x = B[p][col], y = B[q][col];
+            const T rr = sqrt(x * x + y * y);
+            T c = T(1), sn = T(0);
+            if (rr > T(0))
+            {
+                c = x / rr;
+                sn = y / rr;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                const T bp = B[p][k], bq = B[q][k];
+                B[p][k] = c * bp + sn * bq;
+                B[q][k] = -sn * bp + c * bq;
+                const T up = Um[k][p], uq = Um[k][q];
+                Um[k][p] = c * up + sn * uq;
+                Um[k][q] = -sn * up + c * uq;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                U[c * 3 + r] = Um[r][c];
+                V[c * 3 + r] = Vm[r][c];
+            }
+        s[0] = B[0][0];
+        s[1] = B[1][1];
+        s[2] = B[2][2];
+    }
+
+    // Rotation the reference's PB-MPM constraint blends toward: `u * vt` of svd3(targetF), which
+    // factors targetF^T (svd3.h:1271-1274) and therefore equals R^T = V U^T for targetF = U S V^T.
+    // Float first; a near-degenerate spectrum (tiny or nearly equal singular values) is redone
+    // in double precision.
+    __device__ __forceinline__ M3 pbRotationTarget(const M3 &A, unsigned *fp64Count)
+    {
+        float U[9], V[9], s[3];
+        svdRotations<float>(A.m, U, V, s, 5);
+        const float smax = fabsf(s[0]);
+        const bool degenerate = !(fabsf(s[2]) > 1e-3f * smax) || (s[0] - s[1] < 1e-4f * smax) ||
+                                (s[1] - fabsf(s[2]) < 1e-4f * smax);
+        M3 R;
+        if (degenerate)
+        {
+            double Ad[9], Ud[9], Vd[9], sd[3];
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                Ad[i] = (double)A.m[i];
+            svdRotations<double>(Ad, Ud, Vd, sd, 12);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    R.m[c * 3 + r] = (float)(Vd[r] * Ud[c] + Vd[3 + r] * Ud[3 + c] + Vd[6 + r] * Ud[6 + c]);
+            if (fp64Count)
+                atomicAdd(fp64Count, 1u);
+        }
+        else
+        {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    R.m[c * 3 + r] = V[r] * U[c] + V[3 + r] * U[3 + c] + V[6 + r] * U[6 + c];
+        }
+        return R;
+    }
+} // namespace crb200

@@ -1,0 +1,136 @@
+// Host-side solver object of the B200 MPM engine.  One Solver stands in for one of the reference's
+// GPU solvers (src/solver/gpu_{mls,pb,standard}_mpm_solver.cu) and honours the MpmSolver interface
+// (include/solver/mpm_solver.h:63-191) through the C ABI in capi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/crmpm_b200.h"
+#include "mpm_device.cuh"
+
+namespace crb200
+{
+    // Grid geometry of one scene.  Nodes are stored block-major: 4x4x4-node blocks of 64 float4
+    // (1 KiB), block (bx, by, bz) at linear index bx + nb.x * (by + nb.y * bz).
+    struct GridGeom
+    {
+        float3 gmin, gmax;
+        float dx, invDx, cellVol;
+        int3 n;  // node counts per dimension
+        int3 nb; // blocks per dimension
+        unsigned blockBase;
+    };
+
+    struct StepParams
+    {
+        GridGeom g;
+        float dt;
+        float3 gravity;
+        float cutoff;
+        int contactModel;
+        int solverType;
+        unsigned numActive;
+        int numShapes;
+    };
+
+    // Device-side sort / bookkeeping header (one per solver).
+    struct SortHeader
+    {
+        unsigned numActiveBlocks;
+        unsigned numTouchedBlocks;
+        unsigned numSorted;
+        unsigned status;
+        unsigned fp64Fallbacks;
+        unsigned shapeFlags;
+        unsigned touchedNodes;
+        unsigned pad;
+    };
+
+    class Solver
+    {
+    public:
+        Solver(int solverType, int numMaxParticles, float cellSize, const float gmin[3], const float gmax[3],
+               cudaStream_t stream);
+        ~Solver();
+
+        int initialize();
+        int step();
+        int stepMany(int n);
+        int computeInitialData(unsigned n, const unsigned *indices);
+        int fetchResults();
+        int advance(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
+        int collectPhaseTimes();
+
+        // configuration (MpmSolver setters / binders)
+        int solverType;
+        int numMaxParticles;
+        GridGeom geom;
+        cudaStream_t stream;
+        float dt = 0.002f; // MpmSolverBase default (mpm_solver_base.h:146)
+        float3 gravity = {0.f, 0.f, 0.f};
+        int iterations = 10; // GpuPbMpmSolver default (gpu_pb_mpm_solver.cuh:53)
+        int contactModel = 0;
+        unsigned numActive = 0;
+        float4 *positionMass = nullptr;
+        float4 *velocity = nullptr;
+        float4 *matParams = nullptr;
+        int *matType = nullptr;
+        unsigned char *activeMask = nullptr;
+        int numShapes = 0;
+        int *shapeIds = nullptr;
+        CrB200ShapeData shapes{};
+        CrB200GeometryData geometries{};
+        CrB200GeometrySdfData sdf{};
+        bool deterministic = false;
+        bool keepCutMasks = false;
+        bool phaseTiming = false;
+        cudaEvent_t phaseEv[5] = {};
+        float phaseMs[4] = {0, 0, 0, 0};
+        int phaseSteps = 0;
+        int markPhase(int k); // record event k when phase timing is on
+
+        bool initialized = false;
+        unsigned configVersion = 0; // bumped by every setter so captured graphs are refreshed
+
+        // solver-owned device state
+        float *F = nullptr;  // 9 planes of numMaxParticles floats, F(r,c) in plane 3c + r
+        float *Cm = nullptr; // APIC matrix, same layout
+        float *V0 = nullptr;
+        float4 *gridA = nullptr; // accumulation grid (zero outside a substep)
+        float4 *gridV = nullptr; // velocity grid
+        float4 *gridF = nullptr; // node force (standard MPM)
+        unsigned *keys = nullptr, *ranks = nullptr, *sortedIds = nullptr;
+        unsigned long long *sortPairs = nullptr;
+        unsigned *blockCount = nullptr, *blockStart = nullptr;
+        unsigned *activeList = nullptr, *touchedList = nullptr;
+        unsigned *tileSums = nullptr;
+        unsigned char *blockFlags = nullptr;
+        GridGeom *dScenes = nullptr;
+        unsigned *cutMasks = nullptr;
+        SortHeader *header = nullptr;
+        ShapeRec *shapeTable = nullptr;
+        unsigned totalBlocks = 0;
+        unsigned numTiles = 0;
+        int persistentCtas = 0;
+
+        cudaGraphExec_t graph = nullptr;
+        unsigned graphVersion = ~0u;
+        int graphKernels = 0;
+
+        StepParams params() const;
+        int launchStep();   // enqueue one step's kernels
+        int sortParticles(const StepParams &p, bool ignoreMask);
+        void gatherShapes();
+    };
+
+    // error plumbing shared by the C ABI
+    void setLastError(const std::string &msg);
+    int cudaFail(cudaError_t e, const char *what);
+    void noteLaunches(uint64_t n);
+    const char *lastError();
+    uint64_t launchCount();
+} // namespace crb200

@@ -1,0 +1,1465 @@
+// sm_100a kernels of the B200 MPM substep engine and the host Solver that launches them.
+//
+// One substep (MLS-MPM; the reference's GpuMlsMpmSolver::step, gpu_mls_mpm_solver.cu:102-109):
+//   1. gatherShapes   scene shapes -> compact table (shapes may change between substeps)
+//   2. bin            per particle: cell key (block-major), warp-aggregated block histogram
+//   3. scan           block offsets, active-block list, touched-block list (3 kernels)
+//   4. scatter        (local cell, id) pairs into block segments
+//   5. blockSort      canonical order inside each block: by local cell, then particle id
+//   6. p2g            one CTA per active block: particles -> shared-memory 6x6x6 node tile ->
+//                     one float4 vector atomic per touched node into the accumulation grid
+//   7. gridUpdate     touched blocks only: momentum -> velocity, SDF contact/friction, domain BC,
+//                     and the accumulation grid is zeroed as it is consumed
+//   8. g2p            particle order: 27-node gather, APIC matrix, advection, push-out, F update
+// PB-MPM runs 6-8 `iterations` times per step plus an integration kernel (gpu_pb_mpm_solver.cu:
+// 102-113); standard MPM carries a node force tile (gpu_standard_mpm_solver.cu:177-184).
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <atomic>
+#include <cmath>
+#include <string>
+
+#include "mpm_engine.cuh"
+
+namespace crb200
+{
+    constexpr unsigned kInvalidKey = 0xFFFFFFFFu;
+    constexpr int kTileEdge = 6;
+    constexpr int kTileNodes = kTileEdge * kTileEdge * kTileEdge;
+    constexpr int kScanTile = 2048; // blocks per scan tile
+    constexpr int kScanThreads = 256;
+    constexpr int kSortCap = 2048; // particles per block sorted in shared memory
+
+    // ---------------------------------------------------------------------------------------
+    // Addressing helpers
+    __device__ __forceinline__ unsigned nodeAddr(const GridGeom &g, int i, int j, int k)
+    {
+        const unsigned b = g.blockBase + (unsigned)((i >> 2) + g.nb.x * ((j >> 2) + g.nb.y * (k >> 2)));
+        return b * 64u + (unsigned)((i & 3) + 4 * ((j & 3) + 4 * (k & 3)));
+    }
+    __device__ __forceinline__ bool inGrid(const GridGeom &g, int i, int j, int k)
+    {
+        return i >= 0 && i < g.n.x && j >= 0 && j < g.n.y && k >= 0 && k < g.n.z;
+    }
+
+    struct Stencil
+    {
+        int b[3];
+        V3 fx;
+        bool finite;
+    };
+
+    // baseCoord / fx of mls_mpm_algorithm.h:170-175, exactly rounded.
+    __device__ __forceinline__ Stencil stencilOf(const GridGeom &g, V3 x)
+    {
+        Stencil s;
+        const float sp[3] = {ex::mul(ex::sub(x.x, g.gmin.x), g.invDx), ex::mul(ex::sub(x.y, g.gmin.y), g.invDx),
+                             ex::mul(ex::sub(x.z, g.gmin.z), g.invDx)};
+        s.finite = fabsf(sp[0]) < 1.0e7f && fabsf(sp[1]) < 1.0e7f && fabsf(sp[2]) < 1.0e7f;
+        float f[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            s.b[d] = s.finite ? __float2int_rz(ex::sub(sp[d], 0.5f)) : 0;
+            f[d] = ex::sub(sp[d], (float)s.b[d]);
+        }
+        s.fx = v3(f[0], f[1], f[2]);
+        return s;
+    }
+
+    // Quadratic B-spline weights (shape_functions.h:44-57) and gradients (:62-75).
+    __device__ __forceinline__ void weights(V3 fx, float w[3][3])
+    {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            const float f = comp(fx, d);
+            const float a = 1.5f - f, b = f - 1.0f, c = f - 0.5f;
+            w[0][d] = 0.5f * (a * a);
+            w[1][d] = 0.75f - b * b;
+            w[2][d] = 0.5f * (c * c);
+        }
+    }
+    __device__ __forceinline__ void weightGrads(V3 fx, float dw[3][3])
+    {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            const float f = comp(fx, d);
+            dw[0][d] = f - 1.5f;
+            dw[1][d] = 2.0f * (1.0f - f);
+            dw[2][d] = f - 0.5f;
+        }
+    }
+
+    // Sort key: block-major cell index of the clamped base cell; outliers (a base outside the
+    // grid) are binned at the nearest cell, where the P2G tile still covers every in-grid node
+    // of their stencil.
+    __device__ __forceinline__ unsigned cellKey(const GridGeom &g, const Stencil &s, bool *outOfDomain)
+    {
+        int c[3];
+        const int hi[3] = {g.n.x - 2, g.n.y - 2, g.n.z - 2};
+        bool ood = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            c[d] = min(max(s.b[d], 0), max(hi[d], 0));
+            ood |= (c[d] != s.b[d]);
+        }
+        *outOfDomain = ood;
+        const unsigned blk = g.blockBase + (unsigned)((c[0] >> 2) + g.nb.x * ((c[1] >> 2) + g.nb.y * (c[2] >> 2)));
+        return blk * 64u + (unsigned)((c[0] & 3) + 4 * ((c[1] & 3) + 4 * (c[2] & 3)));
+    }
+
+    __device__ __forceinline__ void loadM3(const float *planes, unsigned stride, unsigned i, M3 &m)
+    {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            m.m[k] = planes[k * stride + i];
+    }
+    __device__ __forceinline__ void storeM3(float *planes, unsigned stride, unsigned i, const M3 &m)
+    {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            planes[k * stride + i] = m.m[k];
+    }
+
+    __device__ __forceinline__ void loadShapes(ShapeRec *dst, const ShapeRec *src, int num)
+    {
+        const int words = num * (int)(sizeof(ShapeRec) / sizeof(float4));
+        const float4 *s = reinterpret_cast<const float4 *>(src);
+        float4 *d = reinterpret_cast<float4 *>(dst);
+        for (int t = threadIdx.x; t < words; t += blockDim.x)
+            d[t] = s[t];
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // 1. Shape table
+    __global__ void k_gatherShapes(int num, const int *__restrict__ shapeIds, CrB200ShapeData sh, CrB200GeometryData ge,
+                                   ShapeRec *__restrict__ out, SortHeader *hdr)
+    {
+        __shared__ int flags;
+        if (threadIdx.x == 0)
+            flags = 0;
+        __syncthreads();
+        for (int s = threadIdx.x; s < num; s += blockDim.x)
+        {
+            const int id = shapeIds[s];
+            const int gid = sh.geometryIdx[id];
+            ShapeRec r;
+            r.pos = reinterpret_cast<const float4 *>(sh.position)[id];
+            r.rot = reinterpret_cast<const float4 *>(sh.rotation)[id];
+            r.invScale = reinterpret_cast<const float4 *>(sh.invScale)[id];
+            r.linVel = reinterpret_cast<const float4 *>(sh.linearVelocity)[id];
+            r.angVel = reinterpret_cast<const float4 *>(sh.angularVelocity)[id];
+            r.params0 = reinterpret_cast<const float4 *>(sh.params0)[id];
+            r.gparams = reinterpret_cast<const float4 *>(ge.params0)[gid];
+            r.comInvMass = sh.comInvMass ? reinterpret_cast<const float4 *>(sh.comInvMass)[id] : make_float4(0, 0, 0, 0);
+            r.inertia0 = sh.inertiaInv0 ? reinterpret_cast<const float4 *>(sh.inertiaInv0)[id] : make_float4(0, 0, 0, 0);
+            r.inertia1 = sh.inertiaInv1 ? reinterpret_cast<const float4 *>(sh.inertiaInv1)[id] : make_float4(0, 0, 0, 0);
+            r.kind = sh.type[id];
+            r.gtype = ge.type[gid];
+            r.id = id;
+            r.pad = 0;
+            out[s] = r;
+            int f = 0;
+            if (r.gtype == G_QUAD_SLICER || r.gtype == G_TRIMESH_SLICER)
+                f |= SF_SLICER;
+            if (r.kind == S_DYNAMIC)
+                f |= SF_DYNAMIC;
+            atomicOr(&flags, f);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            hdr->shapeFlags = (unsigned)flags;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // 2. Bin: cell keys and warp-aggregated block histogram (rank = arrival order in its block).
+    __global__ void k_bin(GridGeom g, unsigned numActive, bool ignoreMask, const float4 *__restrict__ xm,
+                          const unsigned char *__restrict__ mask, unsigned *__restrict__ keys,
+                          unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount, SortHeader *hdr)
+    {
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        const unsigned lane = threadIdx.x & 31;
+        unsigned key = kInvalidKey;
+        bool ood = false;
+        if (i < numActive && (ignoreMask || mask[i]))
+        {
+            const float4 x = xm[i];
+            const Stencil s = stencilOf(g, v3(x));
+            if (s.finite)
+                key = cellKey(g, s, &ood);
+            else
+                ood = true;
+        }
+        const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
+        const unsigned peers = __match_any_sync(0xffffffffu, blk);
+        const int leader = __ffs(peers) - 1;
+        unsigned base = 0;
+        if (blk != kInvalidKey && (int)lane == leader)
+            base = atomicAdd(&blockCount[blk], (unsigned)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (i < numActive)
+        {
+            keys[i] = key;
+            ranks[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+        }
+        if (__any_sync(0xffffffffu, ood) && lane == 0)
+            atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // 3. Scan over blocks.  Tile t covers blocks [t*kScanTile, (t+1)*kScanTile).
+    //    flags bit 0: block holds particles; bit 1: block holds nodes some particle touches
+    //    (the block itself or one of its -x/-y/-z neighbours holds particles).
+    __device__ __forceinline__ const GridGeom &sceneOfBlock(const GridGeom *scenes, int numScenes, unsigned b)
+    {
+        int lo = 0, hi = numScenes - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (scenes[mid].blockBase <= b)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return scenes[lo];
+    }
+
+    __global__ void k_scanReduce(const GridGeom *__restrict__ scenes, int numScenes, unsigned totalBlocks,
+                                 const unsigned *__restrict__ blockCount, unsigned char *__restrict__ flags,
+                                 uint3 *__restrict__ tileSums)
+    {
+        unsigned sum = 0, act = 0, tch = 0;
+        const unsigned b0 = blockIdx.x * kScanTile + threadIdx.x * (kScanTile / kScanThreads);
+        for (int e = 0; e < kScanTile / kScanThreads; ++e)
+        {
+            const unsigned b = b0 + e;
+            if (b >= totalBlocks)
+                break;
+            const GridGeom &g = sceneOfBlock(scenes, numScenes, b);
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            const unsigned c = blockCount[b];
+            bool touched = false;
+            for (int d = 0; d < 8 && !touched; ++d)
+            {
+                const int x = bx - (d & 1), y = by - ((d >> 1) & 1), z = bz - (d >> 2);
+                if (x < 0 || y < 0 || z < 0)
+                    continue;
+                touched = blockCount[g.blockBase + x + g.nb.x * (y + g.nb.y * z)] > 0;
+            }
+            flags[b] = (unsigned char)((c > 0 ? 1 : 0) | (touched ? 2 : 0));
+            sum += c;
+            act += c > 0;
+            tch += touched;
+        }
+        // block reduction
+        __shared__ unsigned red[3][kScanThreads / 32];
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            sum += __shfl_down_sync(0xffffffffu, sum, o);
+            act += __shfl_down_sync(0xffffffffu, act, o);
+            tch += __shfl_down_sync(0xffffffffu, tch, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            red[0][threadIdx.x >> 5] = sum;
+            red[1][threadIdx.x >> 5] = act;
+            red[2][threadIdx.x >> 5] = tch;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            uint3 t = make_uint3(0, 0, 0);
+            for (int w = 0; w < kScanThreads / 32; ++w)
+            {
+                t.x += red[0][w];
+                t.y += red[1][w];
+                t.z += red[2][w];
+            }
+            tileSums[blockIdx.x] = t;
+        }
+    }
+
+    // Exclusive scan of the tile sums (single CTA) + totals into the header.
+    __global__ void k_scanTiles(uint3 *__restrict__ tileSums, unsigned numTiles, SortHeader *hdr)
+    {
+        __shared__ uint3 carry;
+        __shared__ uint3 warpTot[32];
+        if (threadIdx.x == 0)
+            carry = make_uint3(0, 0, 0);
+        __syncthreads();
+        for (unsigned base = 0; base < numTiles; base += blockDim.x)
+        {
+            const unsigned t = base + threadIdx.x;
+            uint3 v = t < numTiles ? tileSums[t] : make_uint3(0, 0, 0);
+            uint3 inc = v;
+            const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const unsigned a = __shfl_up_sync(0xffffffffu, inc.x, o), b = __shfl_up_sync(0xffffffffu, inc.y, o),
+                               c = __shfl_up_sync(0xffffffffu, inc.z, o);
+                if (lane >= (unsigned)o)
+                {
+                    inc.x += a;
+                    inc.y += b;
+                    inc.z += c;
+                }
+            }
+            if (lane == 31)
+                warpTot[w] = inc;
+            __syncthreads();
+            if (w == 0)
+            {
+                uint3 x = lane < (blockDim.x >> 5) ? warpTot[lane] : make_uint3(0, 0, 0);
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const unsigned a = __shfl_up_sync(0xffffffffu, x.x, o), b = __shfl_up_sync(0xffffffffu, x.y, o),
+                                   c = __shfl_up_sync(0xffffffffu, x.z, o);
+                    if (lane >= (unsigned)o)
+                    {
+                        x.x += a;
+                        x.y += b;
+                        x.z += c;
+                    }
+                }
+                warpTot[lane] = x; // inclusive over warps
+            }
+            __syncthreads();
+            const uint3 wprev = w > 0 ? warpTot[w - 1] : make_uint3(0, 0, 0);
+            const uint3 c = carry;
+            if (t < numTiles)
+                tileSums[t] = make_uint3(c.x + wprev.x + inc.x - v.x, c.y + wprev.y + inc.y - v.y, c.z + wprev.z + inc.z - v.z);
+            __syncthreads();
+            if (threadIdx.x == blockDim.x - 1)
+            {
+                const uint3 tot = warpTot[(blockDim.x >> 5) - 1];
+                carry = make_uint3(c.x + tot.x, c.y + tot.y, c.z + tot.z);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+        {
+            hdr->numSorted = carry.x;
+            hdr->numActiveBlocks = carry.y;
+            hdr->numTouchedBlocks = carry.z;
+            hdr->touchedNodes = 0;
+        }
+    }
+
+    __global__ void k_scanWrite(unsigned totalBlocks, const uint3 *__restrict__ tileOffsets,
+                                unsigned *__restrict__ blockCount, const unsigned char *__restrict__ flags,
+                                unsigned *__restrict__ blockStart, unsigned *__restrict__ activeList,
+                                unsigned *__restrict__ touchedList)
+    {
+        constexpr int per = kScanTile / kScanThreads;
+        const unsigned b0 = blockIdx.x * kScanTile + threadIdx.x * per;
+        unsigned cnt[per];
+        unsigned char fl[per];
+        unsigned sum = 0, act = 0, tch = 0;
+#pragma unroll
+        for (int e = 0; e < per; ++e)
+        {
+            const unsigned b = b0 + e;
+            cnt[e] = b < totalBlocks ? blockCount[b] : 0;
+            fl[e] = b < totalBlocks ? flags[b] : 0;
+            sum += cnt[e];
+            act += fl[e] & 1;
+            tch += (fl[e] >> 1) & 1;
+        }
+        // block exclusive scan of (sum, act, tch)
+        __shared__ uint3 warpTot[kScanThreads / 32];
+        const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        uint3 inc = make_uint3(sum, act, tch);
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const unsigned a = __shfl_up_sync(0xffffffffu, inc.x, o), b = __shfl_up_sync(0xffffffffu, inc.y, o),
+                           c = __shfl_up_sync(0xffffffffu, inc.z, o);
+            if (lane >= (unsigned)o)
+            {
+                inc.x += a;
+                inc.y += b;
+                inc.z += c;
+            }
+        }
+        if (lane == 31)
+            warpTot[w] = inc;
+        __syncthreads();
+        uint3 wp = make_uint3(0, 0, 0);
+        for (unsigned k = 0; k < w; ++k)
+        {
+            wp.x += warpTot[k].x;
+            wp.y += warpTot[k].y;
+            wp.z += warpTot[k].z;
+        }
+        const uint3 to = tileOffsets[blockIdx.x];
+        unsigned s = to.x + wp.x + inc.x - sum, a = to.y + wp.y + inc.y - act, t = to.z + wp.z + inc.z - tch;
+#pragma unroll
+        for (int e = 0; e < per; ++e)
+        {
+            const unsigned b = b0 + e;
+            if (b >= totalBlocks)
+                break;
+            blockStart[b] = s;
+            s += cnt[e];
+            if (fl[e] & 1)
+                activeList[a++] = b;
+            if (fl[e] & 2)
+                touchedList[t++] = b;
+            blockCount[b] = 0;
+            if (b == totalBlocks - 1)
+                blockStart[totalBlocks] = s;
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // 4. Scatter (local cell, id) into the block segments.
+    __global__ void k_scatter(unsigned numActive, const unsigned *__restrict__ keys, const unsigned *__restrict__ ranks,
+                              const unsigned *__restrict__ blockStart, unsigned long long *__restrict__ pairs)
+    {
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= numActive)
+            return;
+        const unsigned key = keys[i];
+        if (key == kInvalidKey)
+            return;
+        pairs[blockStart[key >> 6] + ranks[i]] = ((unsigned long long)(key & 63u) << 32) | i;
+    }
+
+    // 5. Canonical order inside a block: bitonic sort of (local cell, id) in shared memory; larger
+    //    blocks fall back to a rank sort in global memory.
+    __global__ void __launch_bounds__(256) k_blockSort(const SortHeader *__restrict__ hdr,
+                                                       const unsigned *__restrict__ activeList,
+                                                       const unsigned *__restrict__ blockStart,
+                                                       const unsigned long long *__restrict__ pairs,
+                                                       unsigned *__restrict__ sortedIds, unsigned *status)
+    {
+        __shared__ unsigned long long s[kSortCap];
+        const unsigned nAct = hdr->numActiveBlocks;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
+            if (cnt <= (unsigned)kSortCap)
+            {
+                unsigned P = 1;
+                while (P < cnt)
+                    P <<= 1;
+                for (unsigned t = threadIdx.x; t < P; t += blockDim.x)
+                    s[t] = t < cnt ? pairs[start + t] : ~0ull;
+                __syncthreads();
+                for (unsigned k = 2; k <= P; k <<= 1)
+                {
+                    for (unsigned j = k >> 1; j > 0; j >>= 1)
+                    {
+                        for (unsigned t = threadIdx.x; t < P; t += blockDim.x)
+                        {
+                            const unsigned ixj = t ^ j;
+                            if (ixj > t)
+                            {
+                                const unsigned long long a = s[t], c = s[ixj];
+                                const bool up = (t & k) == 0;
+                                if ((a > c) == up)
+                                {
+                                    s[t] = c;
+                                    s[ixj] = a;
+                                }
+                            }
+                        }
+                        __syncthreads();
+                    }
+                }
+                for (unsigned t = threadIdx.x; t < cnt; t += blockDim.x)
+                    sortedIds[start + t] = (unsigned)s[t];
+                __syncthreads();
+            }
+            else
+            {
+                if (threadIdx.x == 0)
+                    atomicOr(status, CRB200_STATUS_BLOCK_OVERFLOW);
+                for (unsigned t = threadIdx.x; t < cnt; t += blockDim.x)
+                {
+                    const unsigned long long e = pairs[start + t];
+                    unsigned rank = 0;
+                    for (unsigned u = 0; u < cnt; ++u)
+                        rank += pairs[start + u] < e;
+                    sortedIds[start + rank] = (unsigned)e;
+                }
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Particle assignment inside a P2G CTA: lane l of warp w walks a contiguous chunk of the
+    // block's sorted list (chunk length q), so the 32 lanes of a warp sit in different cells and
+    // their shared-memory atomics rarely collide on a node.
+    struct ChunkWalk
+    {
+        unsigned q, lane, warp, nwarps;
+    };
+
+    __device__ __forceinline__ void tileAdd(float *tile, int t, float v) { atomicAdd(&tile[t], v); }
+
+    template <int NV>
+    __device__ __forceinline__ void flushTile(const GridGeom &g, int bx, int by, int bz, float *tile, float4 *gridA,
+                                              float4 *gridF)
+    {
+        for (int t = threadIdx.x; t < kTileNodes; t += blockDim.x)
+        {
+            const int tx = t % kTileEdge, ty = (t / kTileEdge) % kTileEdge, tz = t / (kTileEdge * kTileEdge);
+            const int i = 4 * bx + tx, j = 4 * by + ty, k = 4 * bz + tz;
+            const float m = tile[t], px = tile[kTileNodes + t], py = tile[2 * kTileNodes + t],
+                        pz = tile[3 * kTileNodes + t];
+            if (!inGrid(g, i, j, k))
+                continue;
+            const unsigned a = nodeAddr(g, i, j, k);
+            if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f)
+                atomicAdd(&gridA[a], make_float4(px, py, pz, m));
+            if (NV == 7)
+            {
+                const float fx = tile[4 * kTileNodes + t], fy = tile[5 * kTileNodes + t], fz = tile[6 * kTileNodes + t];
+                if (fx != 0.f || fy != 0.f || fz != 0.f)
+                    atomicAdd(&gridF[a], make_float4(fx, fy, fz, 0.f));
+            }
+        }
+    }
+
+    // 6. P2G.  Mode 0 MLS (mls_mpm_algorithm.h:147-241), 1 PB (pb_mpm_algorithm.h:150-231),
+    //    2 standard (standard_mpm_algorithm.h:146-215).
+    template <int Mode>
+    __global__ void __launch_bounds__(128) k_p2g(StepParams p, const SortHeader *__restrict__ hdr,
+                                                 const unsigned *__restrict__ activeList,
+                                                 const unsigned *__restrict__ blockStart,
+                                                 const unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
+                                                 const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
+                                                 const int *__restrict__ matType, const float *__restrict__ F,
+                                                 float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
+                                                 const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                 float4 *__restrict__ gridA, float4 *__restrict__ gridF,
+                                                 unsigned *fp64Count)
+    {
+        constexpr int NV = Mode == 2 ? 7 : 4;
+        __shared__ float tile[NV * kTileNodes];
+        __shared__ ShapeRec sh[kMaxShapes];
+        const GridGeom &g = p.g;
+        const bool slicers = p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        if (slicers)
+            loadShapes(sh, shapeTable, p.numShapes);
+        const unsigned nAct = hdr->numActiveBlocks;
+        const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            for (int t = threadIdx.x; t < NV * kTileNodes; t += blockDim.x)
+                tile[t] = 0.f;
+            __syncthreads();
+            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
+            const unsigned q = (cnt + 31) / 32;
+            for (unsigned sidx = warp; sidx < q; sidx += nwarps)
+            {
+                const unsigned jj = lane * q + sidx;
+                if (jj >= cnt)
+                    continue;
+                const unsigned id = sortedIds[start + jj];
+                const float4 x4 = xm[id];
+                const V3 x = v3(x4);
+                const float m = x4.w;
+                const Stencil st = stencilOf(g, x);
+                if (!st.finite)
+                    continue;
+                float w[3][3];
+                weights(st.fx, w);
+                const float4 v4 = vel[id];
+                V3 v = v3(v4);
+                M3 Fp, Cp;
+                loadM3(F, stride, id, Fp);
+                if (Mode != 2)
+                    loadM3(Cm, stride, id, Cp);
+                const float4 mp = matParams[id];
+                const int mt = matType[id];
+                // per-particle affine term A (momentum contribution = base + A * d)
+                M3 A;
+                V3 base;
+                float dw[3][3];
+                M3 stress;
+                if (Mode == 0)
+                {
+                    v = v + v3(p.gravity) * p.dt;
+                    stress = kirchhoffStress(Fp, mp.x, mp.y, mt);
+                    const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[id];
+#pragma unroll
+                    for (int e = 0; e < 9; ++e)
+                        A.m[e] = stress.m[e] * coef + Cp.m[e] * m;
+                    base = v * m;
+                }
+                else if (Mode == 1)
+                {
+                    if (mt == 1 || mt == 0)
+                    {
+                        // solveMaterialConstraints (constitutive_models.h:123-156)
+                        M3 tF;
+#pragma unroll
+                        for (int e = 0; e < 9; ++e)
+                            tF.m[e] = Cp.m[e] * p.dt + ((e % 4) == 0 ? 1.f : 0.f);
+                        tF = matmul(tF, Fp);
+                        const M3 R = pbRotationTarget(tF, fp64Count);
+                        const float detF = det3(tF);
+                        const float cd = fminf(fmaxf(fabsf(detF), 0.1f), 1000.0f);
+                        const float qs = 1.0f / (copysignf(1.0f, detF) * sqrtf(cd));
+                        M3 tgt;
+#pragma unroll
+                        for (int e = 0; e < 9; ++e)
+                            tgt.m[e] = R.m[e] * mp.y + (tF.m[e] * qs) * (1.0f - mp.y);
+                        const M3 TF = matmul(tgt, inverse3(Fp));
+#pragma unroll
+                        for (int e = 0; e < 9; ++e)
+                            Cp.m[e] = Cp.m[e] + ((TF.m[e] - ((e % 4) == 0 ? 1.f : 0.f)) - Cp.m[e] * p.dt) * mp.x;
+                        storeM3(Cm, stride, id, Cp);
+                    }
+                    A = Cp;
+                    base = v;
+                }
+                else
+                {
+                    weightGrads(st.fx, dw);
+                    stress = kirchhoffStress(Fp, mp.x, mp.y, mt);
+                }
+                const float v0 = Mode == 2 ? V0[id] : 0.f;
+                const int tb[3] = {st.b[0] - 4 * bx, st.b[1] - 4 * by, st.b[2] - 4 * bz};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                        {
+                            const int ni = st.b[0] + i, nj = st.b[1] + j, nk = st.b[2] + k;
+                            if (!inGrid(g, ni, nj, nk))
+                                continue;
+                            const V3 d = v3(ex::mul(ex::sub((float)i, st.fx.x), g.dx),
+                                            ex::mul(ex::sub((float)j, st.fx.y), g.dx),
+                                            ex::mul(ex::sub((float)k, st.fx.z), g.dx));
+                            if (Mode != 2 && slicers && differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, nullptr))
+                                continue;
+                            const float wt = w[i][0] * w[j][1] * w[k][2];
+                            float vals[7];
+                            if (Mode == 2)
+                            {
+                                const float wm = wt * m;
+                                const V3 gw = v3(dw[i][0] * w[j][1] * w[k][2], w[i][0] * dw[j][1] * w[k][2],
+                                                 w[i][0] * w[j][1] * dw[k][2]);
+                                vals[0] = wm;
+                                vals[1] = v.x * wm;
+                                vals[2] = v.y * wm;
+                                vals[3] = v.z * wm;
+                                const V3 sg = v3(stress.m[0] * gw.x + stress.m[3] * gw.y + stress.m[6] * gw.z,
+                                                 stress.m[1] * gw.x + stress.m[4] * gw.y + stress.m[7] * gw.z,
+                                                 stress.m[2] * gw.x + stress.m[5] * gw.y + stress.m[8] * gw.z);
+                                vals[4] = p.gravity.x * wm + sg.x * (-v0);
+                                vals[5] = p.gravity.y * wm + sg.y * (-v0);
+                                vals[6] = p.gravity.z * wm + sg.z * (-v0);
+                            }
+                            else
+                            {
+                                const V3 ad = v3(A.m[0] * d.x + A.m[3] * d.y + A.m[6] * d.z,
+                                                 A.m[1] * d.x + A.m[4] * d.y + A.m[7] * d.z,
+                                                 A.m[2] * d.x + A.m[5] * d.y + A.m[8] * d.z);
+                                if (Mode == 0)
+                                {
+                                    vals[0] = wt * m;
+                                    vals[1] = (base.x + ad.x) * wt;
+                                    vals[2] = (base.y + ad.y) * wt;
+                                    vals[3] = (base.z + ad.z) * wt;
+                                }
+                                else
+                                {
+                                    // (v + C d) * (w m)  (pb_mpm_algorithm.h:222)
+                                    const float wm = wt * m;
+                                    vals[0] = wm;
+                                    vals[1] = (base.x + ad.x) * wm;
+                                    vals[2] = (base.y + ad.y) * wm;
+                                    vals[3] = (base.z + ad.z) * wm;
+                                }
+                            }
+                            const int tx = tb[0] + i, ty = tb[1] + j, tz = tb[2] + k;
+                            if (tx >= 0 && tx < kTileEdge && ty >= 0 && ty < kTileEdge && tz >= 0 && tz < kTileEdge)
+                            {
+                                const int t = tx + kTileEdge * (ty + kTileEdge * tz);
+#pragma unroll
+                                for (int c = 0; c < NV; ++c)
+                                    tileAdd(tile, c * kTileNodes + t, vals[c]);
+                            }
+                            else
+                            {
+                                const unsigned a = nodeAddr(g, ni, nj, nk);
+                                atomicAdd(&gridA[a], make_float4(vals[1], vals[2], vals[3], vals[0]));
+                                if (Mode == 2)
+                                    atomicAdd(&gridF[a], make_float4(vals[4], vals[5], vals[6], 0.f));
+                            }
+                        }
+            }
+            __syncthreads();
+            flushTile<NV>(g, bx, by, bz, tile, gridA, gridF);
+            __syncthreads();
+        }
+    }
+
+    // 7. Grid update over touched blocks (mls_mpm_algorithm.h:243-294 and its PB / standard twins).
+    __global__ void __launch_bounds__(256) k_gridUpdate(StepParams p, const SortHeader *__restrict__ hdr,
+                                                        const unsigned *__restrict__ touchedList,
+                                                        const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                        float4 *__restrict__ gridA, float4 *__restrict__ gridF,
+                                                        float4 *__restrict__ gridV, float4 *coupleForce,
+                                                        float4 *coupleTorque)
+    {
+        __shared__ ShapeRec sh[kMaxShapes];
+        const GridGeom &g = p.g;
+        if (p.numShapes > 0)
+            loadShapes(sh, shapeTable, p.numShapes);
+        __syncthreads();
+        const unsigned nT = hdr->numTouchedBlocks;
+        const bool withForce = p.solverType == CRB200_SOLVER_GPU_STANDARD;
+        const unsigned perCta = blockDim.x / 64;
+        for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
+        {
+            const unsigned bi = base + threadIdx.x / 64;
+            if (bi >= nT)
+                continue;
+            const unsigned b = touchedList[bi];
+            const unsigned l = threadIdx.x & 63;
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            const int i = 4 * bx + (l & 3), j = 4 * by + ((l >> 2) & 3), k = 4 * bz + (l >> 4);
+            if (!inGrid(g, i, j, k))
+                continue;
+            const unsigned a = b * 64u + l;
+            float4 acc = gridA[a];
+            gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (withForce)
+            {
+                f = gridF[a];
+                gridF[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            {
+                // nodes that received mass (roofline bookkeeping), one atomic per warp
+                const unsigned am = __activemask();
+                const unsigned hit = __ballot_sync(am, acc.w > 0.f);
+                if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1) && hit)
+                    atomicAdd(&const_cast<SortHeader *>(hdr)->touchedNodes, (unsigned)__popc(hit));
+            }
+            if (acc.w < p.cutoff)
+            {
+                gridV[a] = acc; // light nodes keep momentum, which G2P then reads (reference Q2)
+                continue;
+            }
+            if (withForce)
+            {
+                acc.x += f.x * p.dt;
+                acc.y += f.y * p.dt;
+                acc.z += f.z * p.dt;
+            }
+            V3 v = v3(acc.x / acc.w, acc.y / acc.w, acc.z / acc.w);
+            V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z);
+            pos = pos + v * p.dt;
+            if (p.numShapes > 0)
+                rigidContact<false>(v, acc.w, pos, sh, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque);
+            if (i < 2 || i > g.n.x - 3)
+                v.x = 0.f;
+            if (j < 2 || j > g.n.y - 3)
+                v.y = 0.f;
+            if (k < 2 || k > g.n.z - 3)
+                v.z = 0.f;
+            gridV[a] = make_float4(v.x, v.y, v.z, acc.w);
+        }
+    }
+
+    // 8. G2P in particle order.  Mode 0 MLS (mls_mpm_algorithm.h:296-390), 1 PB
+    //    (pb_mpm_algorithm.h:286-361, v and C only), 2 standard (standard_mpm_algorithm.h:274-352).
+    template <int Mode>
+    __global__ void __launch_bounds__(128) k_g2p(StepParams p, const SortHeader *__restrict__ hdr,
+                                                 float4 *__restrict__ xm, float4 *__restrict__ vel,
+                                                 const unsigned char *__restrict__ mask, float *__restrict__ F,
+                                                 float *__restrict__ Cm, unsigned stride,
+                                                 const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                 const float4 *__restrict__ gridV, unsigned *status)
+    {
+        __shared__ ShapeRec sh[kMaxShapes];
+        const GridGeom &g = p.g;
+        if (p.numShapes > 0)
+            loadShapes(sh, shapeTable, p.numShapes);
+        __syncthreads();
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= p.numActive || !mask[i])
+            return;
+        const bool slicers = Mode != 2 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const float4 x4 = xm[i];
+        const V3 x = v3(x4);
+        const Stencil st = stencilOf(g, x);
+        float w[3][3], dw[3][3];
+        weights(st.fx, w);
+        if (Mode == 2)
+            weightGrads(st.fx, dw);
+        V3 vk = v3(0.f, 0.f, 0.f);
+        if (slicers)
+        {
+            vk = v3(vel[i]);
+            if (Mode == 0)
+                vk = vk + v3(p.gravity) * p.dt; // the velocity P2G kicked (mls_mpm_algorithm.h:178)
+        }
+        V3 va = v3(0.f, 0.f, 0.f);
+        float Ca[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            Ca[e] = 0.f;
+        if (st.finite)
+        {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                        if (!inGrid(g, ni, nj, nk))
+                            continue;
+                        const float4 gv = __ldg(&gridV[nodeAddr(g, ni, nj, nk)]);
+                        V3 nv = v3(gv);
+                        const float wt = w[a][0] * w[b][1] * w[c][2];
+                        if (Mode == 2)
+                        {
+                            va = va + nv * wt;
+                            const V3 gw = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2],
+                                             w[a][0] * w[b][1] * dw[c][2]);
+                            // gradientVelocity += gw.outerProduct(nv): M(r, c) = gw_c * nv_r
+#pragma unroll
+                            for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                                for (int rr = 0; rr < 3; ++rr)
+                                    Ca[cc * 3 + rr] += comp(gw, cc) * comp(nv, rr);
+                        }
+                        else
+                        {
+                            const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx),
+                                            ex::mul(ex::sub((float)b, st.fx.y), g.dx),
+                                            ex::mul(ex::sub((float)c, st.fx.z), g.dx));
+                            if (slicers)
+                            {
+                                V3 nrm;
+                                if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, &nrm))
+                                    nv = vk - nrm * dot(vk, nrm) * 2.0f;
+                            }
+                            const V3 nw = nv * wt;
+                            va = va + nw;
+                            // outerProduct(nw, d): M(r, c) = nw_c * d_r
+#pragma unroll
+                            for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                                for (int rr = 0; rr < 3; ++rr)
+                                    Ca[cc * 3 + rr] += comp(nw, cc) * comp(d, rr);
+                        }
+                    }
+        }
+        M3 Cn;
+        const float s4 = 4.f * g.invDx;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            Cn.m[e] = Mode == 2 ? Ca[e] : Ca[e] * s4;
+        if (Mode == 1)
+        {
+            vel[i] = make_float4(va.x, va.y, va.z, 0.f);
+            storeM3(Cm, stride, i, Cn);
+            return;
+        }
+        V3 xn = x + va * p.dt;
+        xn = v3(fminf(fmaxf(xn.x, g.gmin.x), g.gmax.x), fminf(fmaxf(xn.y, g.gmin.y), g.gmax.y),
+                fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
+        V3 vn = va;
+        if (p.numShapes > 0)
+            rigidContact<true>(vn, x4.w, xn, sh, p.numShapes, sdf, false, nullptr, nullptr);
+        M3 Fp, Mu;
+        loadM3(F, stride, i, Fp);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            Mu.m[e] = ((e % 4) == 0 ? 1.f : 0.f) + Cn.m[e] * p.dt;
+        Fp = matmul(Mu, Fp);
+        xm[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
+        vel[i] = make_float4(vn.x, vn.y, vn.z, 0.f);
+        storeM3(F, stride, i, Fp);
+        if (Mode == 0)
+            storeM3(Cm, stride, i, Cn);
+        if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)))
+            atomicOr(status, CRB200_STATUS_NAN_STATE);
+    }
+
+    // PB-MPM integration (pb_mpm_algorithm.h:363-408).
+    __global__ void __launch_bounds__(128) k_pbIntegrate(StepParams p, float4 *__restrict__ xm, float4 *__restrict__ vel,
+                                                         const unsigned char *__restrict__ mask, float *__restrict__ F,
+                                                         const float *__restrict__ Cm, unsigned stride,
+                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                         unsigned *status)
+    {
+        __shared__ ShapeRec sh[kMaxShapes];
+        const GridGeom &g = p.g;
+        if (p.numShapes > 0)
+            loadShapes(sh, shapeTable, p.numShapes);
+        __syncthreads();
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= p.numActive || !mask[i])
+            return;
+        const float4 x4 = xm[i];
+        V3 v = v3(vel[i]);
+        V3 xn = v3(x4) + v * p.dt;
+        xn = v3(fminf(fmaxf(xn.x, g.gmin.x), g.gmax.x), fminf(fmaxf(xn.y, g.gmin.y), g.gmax.y),
+                fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
+        v = v + v3(p.gravity) * p.dt;
+        if (p.numShapes > 0)
+            rigidContact<true>(v, x4.w, xn, sh, p.numShapes, sdf, false, nullptr, nullptr);
+        M3 Fp, Cp, Mu;
+        loadM3(F, stride, i, Fp);
+        loadM3(Cm, stride, i, Cp);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            Mu.m[e] = ((e % 4) == 0 ? 1.f : 0.f) + Cp.m[e] * p.dt;
+        Fp = matmul(Mu, Fp);
+        xm[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
+        vel[i] = make_float4(v.x, v.y, v.z, 0.f);
+        storeM3(F, stride, i, Fp);
+        if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(v.x) && isfinite(v.y) && isfinite(v.z)))
+            atomicOr(status, CRB200_STATUS_NAN_STATE);
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // computeInitialData (mls_mpm_algorithm.h:46-145): F = I, mass scatter, volume gather, then the
+    // accumulation grid is cleared again.
+    __global__ void k_initMass(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+                               float *__restrict__ F, unsigned stride, float4 *__restrict__ gridA)
+    {
+        const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ii >= n)
+            return;
+        const unsigned p = idx[ii];
+        M3 I;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            I.m[e] = (e % 4) == 0 ? 1.f : 0.f;
+        storeM3(F, stride, p, I);
+        const float4 x4 = xm[p];
+        const Stencil st = stencilOf(g, v3(x4));
+        if (!st.finite)
+            return;
+        float w[3][3];
+        weights(st.fx, w);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c)
+                {
+                    const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                    if (!inGrid(g, ni, nj, nk))
+                        continue;
+                    atomicAdd(&gridA[nodeAddr(g, ni, nj, nk)].w, (w[a][0] * w[b][1] * w[c][2]) * x4.w);
+                }
+    }
+
+    __global__ void k_initVolume(GridGeom g, unsigned n, const unsigned *__restrict__ idx,
+                                 const float4 *__restrict__ xm, const float4 *__restrict__ gridA, float *__restrict__ V0)
+    {
+        const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ii >= n)
+            return;
+        const unsigned p = idx[ii];
+        const float4 x4 = xm[p];
+        const Stencil st = stencilOf(g, v3(x4));
+        float dens = 0.f;
+        if (st.finite)
+        {
+            float w[3][3];
+            weights(st.fx, w);
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                        if (!inGrid(g, ni, nj, nk))
+                            continue;
+                        dens += (gridA[nodeAddr(g, ni, nj, nk)].w / g.cellVol) * (w[a][0] * w[b][1] * w[c][2]);
+                    }
+        }
+        V0[p] = dens > 1e-8f ? x4.w / dens : 1e-8f;
+    }
+
+    __global__ void k_initClear(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+                                float4 *__restrict__ gridA)
+    {
+        const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ii >= n)
+            return;
+        const Stencil st = stencilOf(g, v3(xm[idx[ii]]));
+        if (!st.finite)
+            return;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c)
+                {
+                    const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                    if (inGrid(g, ni, nj, nk))
+                        gridA[nodeAddr(g, ni, nj, nk)] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+    }
+
+    // Cut masks of the current positions (bit a*9 + b*3 + c), for inspection.
+    __global__ void k_cutMasks(StepParams p, const SortHeader *__restrict__ hdr, const float4 *__restrict__ xm,
+                               const unsigned char *__restrict__ mask, const ShapeRec *__restrict__ shapeTable,
+                               SdfPtrs sdf, unsigned *__restrict__ out)
+    {
+        __shared__ ShapeRec sh[kMaxShapes];
+        const GridGeom &g = p.g;
+        if (p.numShapes > 0)
+            loadShapes(sh, shapeTable, p.numShapes);
+        __syncthreads();
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= p.numActive)
+            return;
+        unsigned msk = 0;
+        const V3 x = v3(xm[i]);
+        const Stencil st = stencilOf(g, x);
+        if (st.finite && p.numShapes > 0 && p.solverType != CRB200_SOLVER_GPU_STANDARD && mask[i])
+        {
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        if (!inGrid(g, st.b[0] + a, st.b[1] + b, st.b[2] + c))
+                            continue;
+                        const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
+                                        ex::mul(ex::sub((float)c, st.fx.z), g.dx));
+                        if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, nullptr))
+                            msk |= 1u << (a * 9 + b * 3 + c);
+                    }
+        }
+        out[i] = msk;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Host side
+    static thread_local std::string g_lastError;
+    static std::atomic<uint64_t> g_launches{0};
+
+    void setLastError(const std::string &msg) { g_lastError = msg; }
+    const char *lastError() { return g_lastError.c_str(); }
+    void noteLaunches(uint64_t n) { g_launches.fetch_add(n); }
+    uint64_t launchCount() { return g_launches.load(); }
+
+    int cudaFail(cudaError_t e, const char *what)
+    {
+        if (e == cudaSuccess)
+            return CRB200_OK;
+        setLastError(std::string(what) + ": " + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? CRB200_ERR_OUT_OF_MEMORY : CRB200_ERR_CUDA;
+    }
+
+#define CRB_CHECK(call)                                     \
+    do                                                      \
+    {                                                       \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess)                              \
+            return cudaFail(e_, #call);                     \
+    } while (0)
+
+#define CRB_LAUNCHED(n)                                     \
+    do                                                      \
+    {                                                       \
+        noteLaunches(n);                                    \
+        cudaError_t e_ = cudaGetLastError();                \
+        if (e_ != cudaSuccess)                              \
+            return cudaFail(e_, "kernel launch");           \
+    } while (0)
+
+    Solver::Solver(int type, int nmax, float cellSize, const float mn[3], const float mx[3], cudaStream_t s)
+        : solverType(type), numMaxParticles(nmax), stream(s)
+    {
+        // Node counts exactly like the reference constructor (gpu_mls_mpm_solver.cu:40-52):
+        // int((max - min) / dx + 1) in single precision.
+        float dims[3];
+        for (int d = 0; d < 3; ++d)
+        {
+            volatile float size = mx[d] - mn[d];
+            volatile float q = size / cellSize;
+            dims[d] = q + 1.0f;
+        }
+        geom.gmin = make_float3(mn[0], mn[1], mn[2]);
+        geom.gmax = make_float3(mx[0], mx[1], mx[2]);
+        geom.dx = cellSize;
+        geom.invDx = 1 / cellSize;
+        geom.cellVol = cellSize * cellSize * cellSize;
+        geom.n = make_int3((int)dims[0], (int)dims[1], (int)dims[2]);
+        geom.nb = make_int3((geom.n.x + 5) >> 2, (geom.n.y + 5) >> 2, (geom.n.z + 5) >> 2);
+        geom.blockBase = 0;
+        totalBlocks = (unsigned)geom.nb.x * geom.nb.y * geom.nb.z;
+        numTiles = (totalBlocks + kScanTile - 1) / kScanTile;
+    }
+
+    Solver::~Solver()
+    {
+        if (graph)
+            cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : phaseEv)
+            if (e)
+                cudaEventDestroy(e);
+        void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, sortPairs, blockCount, blockStart,
+                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, dScenes};
+        for (void *b : bufs)
+            if (b)
+                cudaFree(b);
+    }
+
+    StepParams Solver::params() const
+    {
+        StepParams p;
+        p.g = geom;
+        p.dt = dt;
+        p.gravity = gravity;
+        p.cutoff = solverType == CRB200_SOLVER_GPU_PB ? 1e-8f : 1e-4f;
+        p.contactModel = contactModel;
+        p.solverType = solverType;
+        p.numActive = numActive;
+        p.numShapes = numShapes;
+        return p;
+    }
+
+    int Solver::initialize()
+    {
+        if (!positionMass || !velocity)
+        {
+            setLastError("initialize: particle data not bound");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        const size_t n = (size_t)numMaxParticles;
+        const size_t nodes = (size_t)totalBlocks * 64;
+        CRB_CHECK(cudaMalloc(&F, 9 * n * sizeof(float)));
+        CRB_CHECK(cudaMalloc(&Cm, 9 * n * sizeof(float)));
+        CRB_CHECK(cudaMalloc(&V0, n * sizeof(float)));
+        CRB_CHECK(cudaMalloc(&gridA, nodes * sizeof(float4)));
+        CRB_CHECK(cudaMalloc(&gridV, nodes * sizeof(float4)));
+        if (solverType == CRB200_SOLVER_GPU_STANDARD)
+            CRB_CHECK(cudaMalloc(&gridF, nodes * sizeof(float4)));
+        CRB_CHECK(cudaMalloc(&keys, n * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&ranks, n * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&sortedIds, n * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&sortPairs, n * sizeof(unsigned long long)));
+        CRB_CHECK(cudaMalloc(&blockCount, (totalBlocks + 1) * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&blockStart, (totalBlocks + 1) * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&activeList, totalBlocks * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&touchedList, totalBlocks * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&tileSums, numTiles * sizeof(uint3)));
+        CRB_CHECK(cudaMalloc(&blockFlags, totalBlocks));
+        CRB_CHECK(cudaMalloc(&dScenes, sizeof(GridGeom)));
+        CRB_CHECK(cudaMemcpyAsync(dScenes, &geom, sizeof(GridGeom), cudaMemcpyHostToDevice, stream));
+        CRB_CHECK(cudaMalloc(&header, sizeof(SortHeader)));
+        CRB_CHECK(cudaMalloc(&shapeTable, kMaxShapes * sizeof(ShapeRec)));
+        CRB_CHECK(cudaMalloc(&cutMasks, n * sizeof(unsigned)));
+        CRB_CHECK(cudaMemsetAsync(F, 0, 9 * n * sizeof(float), stream));
+        CRB_CHECK(cudaMemsetAsync(Cm, 0, 9 * n * sizeof(float), stream));
+        CRB_CHECK(cudaMemsetAsync(V0, 0, n * sizeof(float), stream));
+        CRB_CHECK(cudaMemsetAsync(gridA, 0, nodes * sizeof(float4), stream));
+        CRB_CHECK(cudaMemsetAsync(gridV, 0, nodes * sizeof(float4), stream));
+        if (gridF)
+            CRB_CHECK(cudaMemsetAsync(gridF, 0, nodes * sizeof(float4), stream));
+        CRB_CHECK(cudaMemsetAsync(blockCount, 0, (totalBlocks + 1) * sizeof(unsigned), stream));
+        CRB_CHECK(cudaMemsetAsync(header, 0, sizeof(SortHeader), stream));
+        CRB_CHECK(cudaMemsetAsync(keys, 0xff, n * sizeof(unsigned), stream));
+        int dev = 0, sms = 0, perSm = 0;
+        CRB_CHECK(cudaGetDevice(&dev));
+        CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_p2g<0>, 128, 0));
+        persistentCtas = sms * (perSm > 0 ? perSm : 1);
+        initialized = true;
+        configVersion++;
+        return CRB200_OK;
+    }
+
+    void Solver::gatherShapes()
+    {
+        k_gatherShapes<<<1, 64, 0, stream>>>(numShapes, shapeIds, shapes, geometries, shapeTable, header);
+    }
+
+    int Solver::sortParticles(const StepParams &p, bool ignoreMask)
+    {
+        const unsigned n = numActive;
+        const unsigned pg = (n + 127) / 128;
+        if (n > 0)
+        {
+            k_bin<<<pg, 128, 0, stream>>>(p.g, n, ignoreMask, positionMass, activeMask, keys, ranks, blockCount, header);
+            CRB_LAUNCHED(1);
+        }
+        unsigned char *flags = blockFlags;
+        k_scanReduce<<<numTiles, kScanThreads, 0, stream>>>(dScenes, 1, totalBlocks, blockCount, flags,
+                                                            reinterpret_cast<uint3 *>(tileSums));
+        k_scanTiles<<<1, 1024, 0, stream>>>(reinterpret_cast<uint3 *>(tileSums), numTiles, header);
+        k_scanWrite<<<numTiles, kScanThreads, 0, stream>>>(totalBlocks, reinterpret_cast<const uint3 *>(tileSums),
+                                                           blockCount, flags, blockStart, activeList, touchedList);
+        CRB_LAUNCHED(3);
+        if (n > 0)
+        {
+            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, blockStart, sortPairs);
+            k_blockSort<<<persistentCtas, 256, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds,
+                                                            &header->status);
+            CRB_LAUNCHED(2);
+        }
+        return CRB200_OK;
+    }
+} // namespace crb200
+
+namespace crb200
+{
+    int Solver::launchStep()
+    {
+        if (numShapes > kMaxShapes)
+        {
+            setLastError("step: more than 64 shapes in one scene");
+            return CRB200_ERR_CAPACITY;
+        }
+        if (numShapes > 0 && (!shapeIds || !shapes.type || !geometries.type))
+        {
+            setLastError("step: shapes are enabled but shape ids / shape data / geometry data are not bound");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        const StepParams p = params();
+        markPhase(0);
+        if (numShapes > 0)
+        {
+            gatherShapes();
+            CRB_LAUNCHED(1);
+        }
+        const SdfPtrs sp{reinterpret_cast<const int4 *>(sdf.dimension), reinterpret_cast<const float4 *>(sdf.lowerBoundCellSize),
+                         reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
+        float4 *cf = reinterpret_cast<float4 *>(shapes.force), *ct = reinterpret_cast<float4 *>(shapes.torque);
+        const unsigned stride = (unsigned)numMaxParticles;
+        const unsigned pg = (numActive + 127) / 128;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int updCtas = sms * 8;
+        const bool isStd = solverType == CRB200_SOLVER_GPU_STANDARD;
+        int r = sortParticles(p, isStd);
+        if (r != CRB200_OK)
+            return r;
+        markPhase(1);
+        if (solverType == CRB200_SOLVER_GPU_MLS)
+        {
+            k_p2g<0><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass, velocity,
+                                                         matParams, matType, F, Cm, V0, stride, shapeTable, sp, gridA, gridF,
+                                                         &header->fp64Fallbacks);
+            markPhase(2);
+            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
+            CRB_LAUNCHED(2);
+            markPhase(3);
+            if (pg)
+            {
+                k_g2p<0><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
+                                                 gridV, &header->status);
+                CRB_LAUNCHED(1);
+            }
+        }
+        else if (solverType == CRB200_SOLVER_GPU_PB)
+        {
+            for (int it = 0; it < iterations; ++it)
+            {
+                k_p2g<1><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass,
+                                                             velocity, matParams, matType, F, Cm, V0, stride, shapeTable, sp,
+                                                             gridA, gridF, &header->fp64Fallbacks);
+                if (it == 0)
+                    markPhase(2);
+                k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
+                CRB_LAUNCHED(2);
+                if (it == 0)
+                    markPhase(3);
+                if (pg)
+                {
+                    k_g2p<1><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
+                                                     sp, gridV, &header->status);
+                    CRB_LAUNCHED(1);
+                }
+            }
+            if (pg)
+            {
+                k_pbIntegrate<<<pg, 128, 0, stream>>>(p, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
+                                                      &header->status);
+                CRB_LAUNCHED(1);
+            }
+        }
+        else
+        {
+            k_p2g<2><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass, velocity,
+                                                         matParams, matType, F, Cm, V0, stride, shapeTable, sp, gridA, gridF,
+                                                         &header->fp64Fallbacks);
+            markPhase(2);
+            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
+            CRB_LAUNCHED(2);
+            markPhase(3);
+            if (pg)
+            {
+                k_g2p<2><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
+                                                 gridV, &header->status);
+                CRB_LAUNCHED(1);
+            }
+        }
+        markPhase(4);
+        if (keepCutMasks && pg)
+        {
+            k_cutMasks<<<pg, 128, 0, stream>>>(p, header, positionMass, activeMask, shapeTable, sp, cutMasks);
+            CRB_LAUNCHED(1);
+        }
+        if (phaseTiming)
+            return collectPhaseTimes();
+        return CRB200_OK;
+    }
+
+    // Phase events (PB-MPM folds all iterations' P2G / update / G2P into phases 1-3 by recording the
+    // boundaries of the first iteration only and scaling; see collectPhaseTimes).
+    int Solver::markPhase(int k)
+    {
+        if (!phaseTiming)
+            return CRB200_OK;
+        if (!phaseEv[k])
+            CRB_CHECK(cudaEventCreate(&phaseEv[k]));
+        CRB_CHECK(cudaEventRecord(phaseEv[k], stream));
+        return CRB200_OK;
+    }
+
+    int Solver::collectPhaseTimes()
+    {
+        CRB_CHECK(cudaEventSynchronize(phaseEv[4]));
+        for (int k = 0; k < 4; ++k)
+        {
+            float ms = 0.f;
+            CRB_CHECK(cudaEventElapsedTime(&ms, phaseEv[k], phaseEv[k + 1]));
+            phaseMs[k] += ms;
+        }
+        phaseSteps++;
+        return CRB200_OK;
+    }
+
+    int Solver::advance(float dtFrame, float4 *hostX, float4 *hostV, int *outSubsteps)
+    {
+        // scene_impl.cpp:313-317: float time accumulation decides the substep count
+        float t = 0.f;
+        int n = 0;
+        while (t < dtFrame)
+        {
+            t += dt;
+            ++n;
+        }
+        int r = stepMany(n);
+        if (r != CRB200_OK)
+            return r;
+        if (hostX && numActive)
+            CRB_CHECK(cudaMemcpyAsync(hostX, positionMass, numActive * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        if (hostV && numActive)
+            CRB_CHECK(cudaMemcpyAsync(hostV, velocity, numActive * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        CRB_CHECK(cudaStreamSynchronize(stream));
+        if (outSubsteps)
+            *outSubsteps = n;
+        return CRB200_OK;
+    }
+
+    int Solver::step()
+    {
+        if (!initialized)
+        {
+            setLastError("step: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        return launchStep();
+    }
+
+    int Solver::stepMany(int n)
+    {
+        if (!initialized)
+        {
+            setLastError("stepMany: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        if (n <= 0)
+            return CRB200_OK;
+        if (stream == nullptr || n < 2 || phaseTiming)
+        {
+            for (int i = 0; i < n; ++i)
+            {
+                int r = launchStep();
+                if (r != CRB200_OK)
+                    return r;
+            }
+            return CRB200_OK;
+        }
+        if (graph == nullptr || graphVersion != configVersion)
+        {
+            if (graph)
+            {
+                cudaGraphExecDestroy(graph);
+                graph = nullptr;
+            }
+            const uint64_t before = launchCount();
+            CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            int r = launchStep();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            const uint64_t captured = launchCount() - before;
+            noteLaunches((uint64_t)0 - captured); // captured, not yet executed
+            if (r != CRB200_OK)
+            {
+                if (g)
+                    cudaGraphDestroy(g);
+                return r;
+            }
+            if (e != cudaSuccess)
+                return cudaFail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess)
+                return cudaFail(e, "cudaGraphInstantiate");
+            graphKernels = (int)captured;
+            graphVersion = configVersion;
+        }
+        for (int i = 0; i < n; ++i)
+            CRB_CHECK(cudaGraphLaunch(graph, stream));
+        noteLaunches((uint64_t)graphKernels * (uint64_t)n);
+        return CRB200_OK;
+    }
+
+    int Solver::computeInitialData(unsigned n, const unsigned *indices)
+    {
+        if (!initialized)
+        {
+            setLastError("computeInitialData: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        if (n == 0)
+            return CRB200_OK;
+        if (!indices)
+        {
+            setLastError("computeInitialData: null index list");
+            return CRB200_ERR_INVALID_ARGUMENT;
+        }
+        const unsigned g = (n + 127) / 128;
+        k_initMass<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, F, (unsigned)numMaxParticles, gridA);
+        k_initVolume<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, gridA, V0);
+        k_initClear<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, gridA);
+        CRB_LAUNCHED(3);
+        return CRB200_OK;
+    }
+
+    int Solver::fetchResults()
+    {
+        CRB_CHECK(cudaStreamSynchronize(stream));
+        return CRB200_OK;
+    }
+} // namespace crb200

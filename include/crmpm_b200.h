@@ -178,6 +178,14 @@ CRB200_API int CrB200SolverFetchResults(CrB200SolverHandle solver);
 CRB200_API int CrB200SolverComputeInitialData(CrB200SolverHandle solver, unsigned int numParticles,
                                               const unsigned int *indicesDevice);
 
+/* SceneImpl::_advanceTaskFn (src/engine/scene_impl.cpp:308-330): run substeps with the
+ * reference's float accumulation `while (t < dt) t += step()`, then copy positionMass and
+ * velocity of particles [0, numActive) into the host buffers (either may be NULL) as
+ * SceneImpl::afterAdvance does (:249-263), and wait for the stream.  Host buffers should be
+ * pinned for full copy bandwidth.  Writes the number of substeps taken to *outSubsteps. */
+CRB200_API int CrB200SolverAdvance(CrB200SolverHandle solver, float dt, CrB200Float4 *positionMassHost,
+                                   CrB200Float4 *velocityHost, int *outSubsteps);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Setters and binders (MpmSolver, mpm_solver.h:80-184; MpmSolverBase, mpm_solver_base.h)      */
 /* ------------------------------------------------------------------------------------------ */
@@ -248,7 +256,20 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * per-particle slicer masks for CrB200SolverCopyCutMasks. */
 #define CRB200_OPT_DETERMINISTIC 1
 #define CRB200_OPT_CUT_MASKS 2
+#define CRB200_OPT_PHASE_TIMING 3
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
+
+/* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the
+ * solver stream since the last reset, and the number of substeps they cover.  Phases:
+ * 0 shape gather + binning + scan + sort, 1 P2G, 2 grid update, 3 G2P (PB-MPM: G2P plus the
+ * integration kernel).  Synchronizes the solver stream. */
+#define CRB200_NUM_PHASES 4
+CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[CRB200_NUM_PHASES],
+                                         int *outSubsteps, int reset);
+
+/* Grid bookkeeping of the most recent substep: particles binned, active blocks, blocks updated,
+ * and nodes that received mass (the touched-node count of the roofline byte model). */
+CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4]);
 
 #ifdef __cplusplus
 }

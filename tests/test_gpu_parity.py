@@ -1,0 +1,130 @@
+"""Parity of the sm_100a engine (through the C ABI) with the CPU oracles.
+
+Tolerances (float32 kernels vs the FP64 oracle, and vs the reference's own float32 arithmetic):
+positions within 1e-4 of max(displacement, dx) after the full run, velocities within 1e-3 of the
+velocity scale, deformation gradients within 1e-4 absolute.  Integer outputs (cell keys, the sort
+permutation, slicer cut masks) must match bit for bit on identical float inputs.
+"""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from gpu_helpers import block_keys, canonical_permutation, rel_pos_err
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+import crmpm_b200 as cb  # noqa: E402
+import oracle_py as op  # noqa: E402
+from crmpm_b200 import scenes  # noqa: E402
+
+POS_TOL = 1e-4
+F_TOL = 1e-4
+
+
+def _gpu(sc, **kw):
+    cb.build_library()
+    return cb.DeviceScene(sc, **kw)
+
+
+def _compare(sc, steps, ref32=True, pos_tol=POS_TOL, f_tol=F_TOL, v_tol=1e-3):
+    g = _gpu(sc)
+    o64 = op.PortOracle(sc, 64)
+    o64.compute_initial_data()
+    g.step(steps)
+    o64.step(steps)
+    a, b = g.state(), o64.state()
+    x0 = sc.pos_mass[:, :3]
+    e64 = rel_pos_err(a["x"], b["x"], x0, sc.cell_size)
+    assert e64 <= pos_tol, f"position error vs FP64 oracle {e64:.3e}"
+    vscale = max(float(np.abs(b["v"]).max()), 1e-3)
+    assert float(np.abs(a["v"] - b["v"]).max()) <= v_tol * vscale + 1e-6
+    assert float(np.abs(a["F"] - b["F"]).max()) <= f_tol
+    np.testing.assert_allclose(a["V0"], b["V0"], rtol=1e-5)
+    if ref32 and op.ref_available():
+        r = op.RefOracle(sc)
+        r.compute_initial_data()
+        r.step(steps)
+        c = r.state()
+        assert rel_pos_err(a["x"], c["x"], x0, sc.cell_size) <= pos_tol
+    return a, b
+
+
+def test_initial_volume_matches_reference_order_oracle():
+    sc = scenes.cube_drop()
+    g = _gpu(sc)
+    o = op.PortOracle(sc, 32)
+    o.compute_initial_data()
+    a, b = g.state(), o.state()
+    np.testing.assert_allclose(a["V0"], b["V0"], rtol=2e-6)
+    np.testing.assert_array_equal(a["F"], np.tile(np.eye(3).T.ravel(), (sc.n, 1)).astype(np.float32))
+
+
+def test_mls_cube_drop_500_substeps():
+    """The reference's own CPU-runnable case: 4096-particle Neo-Hookean cube onto a plane."""
+    _compare(scenes.cube_drop(), 500)
+
+
+@pytest.mark.parametrize("material", [scenes.MAT_COROTATIONAL, scenes.MAT_LINEAR_ELASTIC])
+def test_mls_materials(material):
+    _compare(scenes.cube_drop(material=material), 200)
+
+
+def test_standard_mpm_cube():
+    _compare(scenes.cube_drop(solver=scenes.SOLVER_STANDARD, dt=1e-4), 200)
+
+
+def test_pb_mpm_cube():
+    sc = scenes.cube_drop(solver=scenes.SOLVER_PB, dt=0.002)
+    sc.mat_params[:, :2] = (1.0, 0.9)
+    sc.iterations = 10
+    _compare(sc, 30, f_tol=2e-4)
+
+
+def test_sort_keys_and_permutation_bitexact():
+    sc = scenes.cube_drop()
+    g = _gpu(sc)
+    for _ in range(3):
+        x_before = g.pos[: sc.n, :3].cpu().numpy()
+        g.step(1, graph=False)
+        keys, ids = g.sort_state()
+        exp = block_keys(sc, x_before)
+        np.testing.assert_array_equal(keys, exp)
+        np.testing.assert_array_equal(ids, canonical_permutation(exp, sc.mask.astype(bool)))
+        g.step(40)
+
+
+def test_inactive_particles_are_skipped():
+    sc = scenes.cube_drop()
+    sc.mask[::7] = 0
+    a, b = _compare(sc, 100)
+    # inactive particles never move
+    np.testing.assert_array_equal(a["x"][::7], sc.pos_mass[::7, :3])
+
+
+def test_tissue_slab_small_with_probe():
+    sc = scenes.tissue_slab(size=(0.2, 0.06, 0.2), cell=0.01, bounds_min=(-0.15, -0.05, -0.15),
+                            bounds_max=(0.15, 0.15, 0.15))
+    _compare(sc, 100)
+
+
+def test_determinism_run_to_run():
+    sc = scenes.cube_drop()
+    runs = []
+    for _ in range(2):
+        g = _gpu(sc)
+        g.step(50)
+        runs.append(g.state())
+    for k in ("x", "v", "F", "C"):
+        # float atomics make the order of node sums vary between runs; differences stay at rounding level
+        assert float(np.abs(runs[0][k] - runs[1][k]).max()) <= 1e-5
+
+
+def test_status_reports_nan_velocity():
+    sc = scenes.cube_drop()
+    sc.vel[10, 0] = np.nan
+    g = _gpu(sc)
+    g.step(2, graph=False)
+    st = g.solver.status()
+    assert st & cb.STATUS_NAN_STATE
+    g.solver.clear_status()
+    assert g.solver.status() == 0
