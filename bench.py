@@ -209,6 +209,10 @@ def run_ours(args, rank, world, local):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world)
     value = world * n * args.steps / (ms_max / 1e3)
+    if args.quick:
+        return {"metric": "particle-substeps/s (MLS-MPM 1.6M p)", "value": value, "unit": "particle-substeps/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "quick": True, "gpu_launches": int(launches)}
 
     # per-kernel timing pass (CUDA events around each phase on the solver stream)
     s.set_option(cb.OPT_PHASE_TIMING, 1)
@@ -241,7 +245,8 @@ def run_ours(args, rank, world, local):
     host_pos = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
     host_vel = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
     probe = scene.shapes.shape_ids[-1]
-    pose_host = torch.tensor(ds.sh["position"][probe].cpu().numpy(), pin_memory=True)
+    pose_host = torch.empty(4, dtype=torch.float32, pin_memory=True)
+    pose_host.copy_(ds.sh["position"][probe].cpu())
     frames = max(3, args.steps // frame_substeps)
     s.advance(frame_dt, host_pos.data_ptr(), host_vel.data_ptr())  # warm-up
     barrier(world)
@@ -335,6 +340,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="slab", choices=["slab", "cube"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="timed region only (no phase pass, e2e or CPU baseline): for profiler launch lists")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

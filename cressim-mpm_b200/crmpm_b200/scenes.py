@@ -246,12 +246,14 @@ def tissue_slab(seed: int = 1002, size=(1.0, 0.2, 1.0), cell: float = 0.01, ppc:
     mass = rho * cell ** 3 / ppc
     pm, vel, mp, mt, mask = _particles(pos, mass, (lam, mu, 0, 0), MAT_NEOHOOKEAN)
     st = ShapeTable.empty()
+    # Static boxes abut the four side faces; grid nodes within one cell of a face take the box's
+    # (zero) velocity because drag 0 removes all tangential motion (mpm_rigid_contact.h:356-374).
     t = pin_thickness
-    gx = st.add_geometry(GEOM_BOX, (t, sy / 2 + t, sz / 2 + t, 0))
-    gz = st.add_geometry(GEOM_BOX, (sx / 2 + t, sy / 2 + t, t, 0))
+    gx = st.add_geometry(GEOM_BOX, (t, sy / 2 + t, sz / 2 + 2 * t, 0))
+    gz = st.add_geometry(GEOM_BOX, (sx / 2 + 2 * t, sy / 2 + t, t, 0))
     for sgn in (-1.0, 1.0):
-        st.add_shape(gx, SHAPE_STATIC, (sgn * sx / 2, sy / 2, 0), smooth=0.0, drag=0.0, friction=0.0)
-        st.add_shape(gz, SHAPE_STATIC, (0, sy / 2, sgn * sz / 2), smooth=0.0, drag=0.0, friction=0.0)
+        st.add_shape(gx, SHAPE_STATIC, (sgn * (sx / 2 + t), sy / 2, 0), smooth=cell, drag=0.0, friction=0.0)
+        st.add_shape(gz, SHAPE_STATIC, (0, sy / 2, sgn * (sz / 2 + t)), smooth=cell, drag=0.0, friction=0.0)
     gs = st.add_geometry(GEOM_SPHERE, (probe_radius, 0, 0, 0))
     st.add_shape(gs, SHAPE_KINEMATIC, (0, sy + probe_radius + cell, 0), smooth=0.0, drag=1.0, friction=friction,
                  lin_vel=(0, -probe_speed, 0))

@@ -1,9 +1,11 @@
 """Parity of the sm_100a engine (through the C ABI) with the CPU oracles.
 
 Tolerances (float32 kernels vs the FP64 oracle, and vs the reference's own float32 arithmetic):
-positions within 1e-4 of max(displacement, dx) after the full run, velocities within 1e-3 of the
-velocity scale, deformation gradients within 1e-4 absolute.  Integer outputs (cell keys, the sort
-permutation, slicer cut masks) must match bit for bit on identical float inputs.
+positions within max(1e-4, 2 x the reference float32 run's own deviation from FP64) of
+max(displacement, dx) after the full run; velocities within 1e-3 of the velocity scale (or twice
+the reference's own deviation); deformation gradients within 1e-4 absolute (same rule).  Integer
+outputs (cell keys, the sort permutation, slicer cut masks) must match bit for bit on identical
+float inputs.
 """
 import numpy as np
 import pytest
@@ -26,26 +28,34 @@ def _gpu(sc, **kw):
     return cb.DeviceScene(sc, **kw)
 
 
-def _compare(sc, steps, ref32=True, pos_tol=POS_TOL, f_tol=F_TOL, v_tol=1e-3):
+def _compare(sc, steps, pos_tol=POS_TOL, f_tol=F_TOL, v_tol=1e-3):
+    """GPU vs the FP64 oracle and vs the reference's float32 arithmetic.
+
+    Contact-heavy scenes are sensitive: the reference's own float32 run drifts from FP64 by more
+    than 1e-4.  The GPU must then stay within twice that drift of FP64 (and of the float32 run).
+    """
     g = _gpu(sc)
     o64 = op.PortOracle(sc, 64)
     o64.compute_initial_data()
+    r32 = op.RefOracle(sc) if op.ref_available() else op.PortOracle(sc, 32)
+    r32.compute_initial_data()
     g.step(steps)
     o64.step(steps)
-    a, b = g.state(), o64.state()
+    r32.step(steps)
+    a, b, c = g.state(), o64.state(), r32.state()
     x0 = sc.pos_mass[:, :3]
+    e_ref = rel_pos_err(c["x"], b["x"], x0, sc.cell_size)
+    tol = max(pos_tol, 2.0 * e_ref)
     e64 = rel_pos_err(a["x"], b["x"], x0, sc.cell_size)
-    assert e64 <= pos_tol, f"position error vs FP64 oracle {e64:.3e}"
+    e32 = rel_pos_err(a["x"], c["x"], x0, sc.cell_size)
+    assert e64 <= tol, f"position error vs FP64 {e64:.3e} (reference float32 vs FP64: {e_ref:.3e})"
+    assert e32 <= tol, f"position error vs reference float32 {e32:.3e} (reference float32 vs FP64: {e_ref:.3e})"
     vscale = max(float(np.abs(b["v"]).max()), 1e-3)
-    assert float(np.abs(a["v"] - b["v"]).max()) <= v_tol * vscale + 1e-6
-    assert float(np.abs(a["F"] - b["F"]).max()) <= f_tol
+    dv_ref = float(np.abs(c["v"] - b["v"]).max())
+    assert float(np.abs(a["v"] - b["v"]).max()) <= max(v_tol * vscale, 2.0 * dv_ref) + 1e-6
+    df_ref = float(np.abs(c["F"] - b["F"]).max())
+    assert float(np.abs(a["F"] - b["F"]).max()) <= max(f_tol, 2.0 * df_ref)
     np.testing.assert_allclose(a["V0"], b["V0"], rtol=1e-5)
-    if ref32 and op.ref_available():
-        r = op.RefOracle(sc)
-        r.compute_initial_data()
-        r.step(steps)
-        c = r.state()
-        assert rel_pos_err(a["x"], c["x"], x0, sc.cell_size) <= pos_tol
     return a, b
 
 
@@ -84,6 +94,7 @@ def test_sort_keys_and_permutation_bitexact():
     sc = scenes.cube_drop()
     g = _gpu(sc)
     for _ in range(3):
+        g.sync()
         x_before = g.pos[: sc.n, :3].cpu().numpy()
         g.step(1, graph=False)
         keys, ids = g.sort_state()
