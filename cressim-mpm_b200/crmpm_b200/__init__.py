@@ -30,8 +30,6 @@ ERR_TIMEOUT = -7
 STATUS_NAN_STATE = 0x1
 STATUS_BLOCK_OVERFLOW = 0x2
 STATUS_OUT_OF_DOMAIN = 0x4
-OPT_DETERMINISTIC = 1
-OPT_CUT_MASKS = 2
 OPT_PHASE_TIMING = 3
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 

@@ -339,3 +339,110 @@ def material_cube(seed: int = 1005, side: float = 0.4, cell: float = 0.02, ppc: 
     st.add_shape(g, SHAPE_STATIC, (0, 0, 0), friction=0.3)
     return Scene(SOLVER_MLS, np.array([-0.5, -0.1, -0.5], np.float32), np.array([0.5, 0.7, 0.5], np.float32),
                  cell, dt, np.array([0, -9.81, 0], np.float32), 20, 0, pm, vel, mp, mt, mask, st, "material_cube")
+
+
+def _sphere_sdf_grid(radius: float, cell: float, margin: int = 3):
+    """Sampled SDF of a sphere on a regular grid: values (float32 [dz,dy,dx,4]) and metadata."""
+    n = int(math.ceil(2 * radius / cell)) + 2 * margin + 1
+    lower = -(n - 1) / 2 * cell
+    ax = lower + np.arange(n) * cell
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    r = np.sqrt(x * x + y * y + z * z)
+    vals = np.zeros((n, n, n, 4), np.float32)
+    rr = np.maximum(r, 1e-9)
+    vals[..., 0] = x / rr
+    vals[..., 1] = y / rr
+    vals[..., 2] = z / rr
+    vals[..., 3] = r - radius
+    return vals, (n, n, n), (lower, lower, lower)
+
+
+def _plane_slicer_grid(half: float, cell: float, thickness_cells: int = 3):
+    """Sampled signed distance of the plane y = 0 over a box (a flat cutting blade)."""
+    nx = int(math.ceil(2 * half / cell)) + 1
+    ny = 2 * thickness_cells + 1
+    lower = (-(nx - 1) / 2 * cell, -thickness_cells * cell, -(nx - 1) / 2 * cell)
+    vals = np.zeros((nx, ny, nx, 4), np.float32)
+    ys = lower[1] + np.arange(ny) * cell
+    vals[..., 1] = 1.0
+    vals[..., 3] = ys[None, :, None]
+    return vals, (nx, ny, nx), lower
+
+
+def contact_scene(kind: str, seed: int = 1010, solver: int = SOLVER_MLS, dt: float = 2e-4) -> Scene:
+    """A small cube (4096 particles) moving onto one rigid geometry of the given kind.
+
+    kinds: box, sphere, plane, capsule, arc, lines, trimesh, quad_slicer, mesh_slicer,
+    dynamic_sphere (coupling force recorded), effmass_sphere (effective-mass contact model),
+    scaled_box (rotated, non-uniformly scaled box).
+    """
+    cell = 0.02
+    h = 0.08
+    pos = jittered_box((-h, 0.12 - h, -h), (h, 0.12 + h, h), cell, 8, seed)
+    lam, mu = lame(2e4, 0.3)
+    pm, vel, mp, mt, mask = _particles(pos, 1000.0 * cell ** 3 / 8, (lam, mu, 0, 0), MAT_NEOHOOKEAN)
+    vel[:, 1] = -1.0
+    st = ShapeTable.empty()
+    contact_model = 0
+    kin = dict(smooth=cell, drag=0.8, friction=0.3)
+    if kind == "box":
+        g = st.add_geometry(GEOM_BOX, (0.06, 0.02, 0.06, 0))
+        st.add_shape(g, SHAPE_STATIC, (0.01, 0.0, -0.01), **kin)
+    elif kind == "scaled_box":
+        g = st.add_geometry(GEOM_BOX, (0.06, 0.02, 0.06, 0))
+        c, s = math.cos(0.2), math.sin(0.2)
+        st.add_shape(g, SHAPE_KINEMATIC, (0.0, 0.0, 0.0), rotation=(0, 0, s, c), inv_scale=(1 / 1.2, 1 / 0.8, 1.0),
+                     lin_vel=(0.1, 0, 0), ang_vel=(0, 0.5, 0), **kin)
+    elif kind == "sphere":
+        g = st.add_geometry(GEOM_SPHERE, (0.05, 0, 0, 0))
+        st.add_shape(g, SHAPE_KINEMATIC, (0.02, -0.01, 0.0), lin_vel=(0, 0.2, 0), **kin)
+    elif kind == "plane":
+        g = st.add_geometry(GEOM_PLANE, (0, 0, 0, 0))
+        c, s = math.cos(0.15), math.sin(0.15)
+        st.add_shape(g, SHAPE_STATIC, (0, 0.01, 0), rotation=(s, 0, 0, c), **kin)
+    elif kind == "capsule":
+        g = st.add_geometry(GEOM_CAPSULE, (0.03, 0.05, 0, 0))
+        c = math.cos(math.pi / 4)
+        st.add_shape(g, SHAPE_STATIC, (0, 0.0, 0), rotation=(0, 0, c, c), **kin)
+    elif kind == "arc":
+        g = st.add_geometry(GEOM_ARC, (-2.5, 2.5, 0, 0))
+        st.add_shape(g, SHAPE_KINEMATIC, (0, 0.06, 0), inv_scale=(1 / 0.07, 1 / 0.07, 1 / 0.07), lin_vel=(0, 0.3, 0),
+                     smooth=0.01, drag=1.0, friction=0.5)
+    elif kind == "lines":
+        pts = np.array([[-0.1, 0.06, -0.05], [-0.03, 0.07, 0.0], [0.03, 0.06, 0.02], [0.1, 0.07, 0.04]], np.float32)
+        lo = pts.min(0) - 0.05
+        hi = pts.max(0) + 0.05
+        vals = np.zeros((len(pts), 4), np.float32)
+        vals[:, :3] = pts
+        header = np.array([[hi[0], hi[1], hi[2], 0]], np.float32)
+        off, sid = st.add_sdf_block((0, 0, 0), lo, 0.0, vals, header=header)
+        g = st.add_geometry(GEOM_CONNECTED_LINE_SEGMENTS, (int_bits(off), int_bits(sid), int_bits(len(pts) + 1), 0))
+        st.add_shape(g, SHAPE_KINEMATIC, (0, 0, 0), lin_vel=(0, 0.2, 0), smooth=0.01, drag=1.0, friction=0.5)
+    elif kind == "trimesh":
+        vals, dims, lower = _sphere_sdf_grid(0.05, 0.01)
+        off, sid = st.add_sdf_block(dims, lower, 0.01, vals)
+        g = st.add_geometry(GEOM_TRIANGLE_MESH, (int_bits(off), int_bits(sid), int_bits(vals.size // 4), 0))
+        st.add_shape(g, SHAPE_STATIC, (0.0, 0.0, 0.01), **kin)
+    elif kind in ("quad_slicer", "mesh_slicer"):
+        if kind == "quad_slicer":
+            g = st.add_geometry(GEOM_QUAD_SLICER, (0.12, 0.12, 0, 0))
+        else:
+            vals, dims, lower = _plane_slicer_grid(0.12, 0.01)
+            spine = np.array([[0.0, 0.0, 1.0, -0.5]], np.float32)  # spine where local z > 0.5 (outside)
+            off, sid = st.add_sdf_block(dims, lower, 0.01, vals, header=spine)
+            g = st.add_geometry(GEOM_TRIANGLE_MESH_SLICER, (int_bits(off), int_bits(sid), int_bits(vals.size // 4 + 1), 0))
+        # blade normal (local y) rotated to world x: the cube is cut along x = 0.003
+        c = math.cos(math.pi / 4)
+        st.add_shape(g, SHAPE_KINEMATIC, (0.003, 0.12, 0.0), rotation=(0, 0, c, c), smooth=0.0, drag=1.0, friction=0.0,
+                     fatten=0.002, lin_vel=(0, -0.2, 0))
+        gp = st.add_geometry(GEOM_PLANE, (0, 0, 0, 0))
+        st.add_shape(gp, SHAPE_STATIC, (0, 0.0, 0), **kin)
+    elif kind in ("dynamic_sphere", "effmass_sphere"):
+        g = st.add_geometry(GEOM_SPHERE, (0.05, 0, 0, 0))
+        st.add_shape(g, SHAPE_DYNAMIC, (0.01, -0.01, 0.0), com_inv_mass=(0.0, 0.0, 0.0, 2.0),
+                     inertia0=(50.0, 50.0, 50.0, 0), inertia1=(1.0, 0.5, 0.2, 0), **kin)
+        contact_model = 1 if kind == "effmass_sphere" else 0
+    else:
+        raise ValueError(kind)
+    return Scene(solver, np.array([-0.3, -0.2, -0.3], np.float32), np.array([0.3, 0.4, 0.3], np.float32), cell, dt,
+                 np.array([0, -9.81, 0], np.float32), 10, contact_model, pm, vel, mp, mt, mask, st, f"contact_{kind}")

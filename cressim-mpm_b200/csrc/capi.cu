@@ -378,11 +378,6 @@ extern "C"
     CRB200_API int CrB200SolverCopyCutMasks(CrB200SolverHandle solver, unsigned int *masks)
     {
         SOLVER_OR_FAIL(solver);
-        if (!s->keepCutMasks)
-        {
-            crb200::setLastError("CrB200SolverCopyCutMasks: enable CRB200_OPT_CUT_MASKS first");
-            return CRB200_ERR_UNSUPPORTED;
-        }
         if (!masks)
             return bad("CrB200SolverCopyCutMasks: null pointer");
         cudaError_t e = cudaMemcpyAsync(masks, s->cutMasks, s->numActive * sizeof(unsigned), cudaMemcpyDeviceToDevice,
@@ -435,11 +430,7 @@ extern "C"
     CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value)
     {
         SOLVER_OR_FAIL(solver);
-        if (option == CRB200_OPT_DETERMINISTIC)
-            s->deterministic = value != 0;
-        else if (option == CRB200_OPT_CUT_MASKS)
-            s->keepCutMasks = value != 0;
-        else if (option == CRB200_OPT_PHASE_TIMING)
+        if (option == CRB200_OPT_PHASE_TIMING)
             s->phaseTiming = value != 0;
         else
             return bad("CrB200SolverSetOption: unknown option");

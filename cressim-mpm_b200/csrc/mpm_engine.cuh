@@ -85,8 +85,6 @@ namespace crb200
         CrB200ShapeData shapes{};
         CrB200GeometryData geometries{};
         CrB200GeometrySdfData sdf{};
-        bool deterministic = false;
-        bool keepCutMasks = false;
         bool phaseTiming = false;
         cudaEvent_t phaseEv[5] = {};
         float phaseMs[4] = {0, 0, 0, 0};
@@ -115,7 +113,8 @@ namespace crb200
         ShapeRec *shapeTable = nullptr;
         unsigned totalBlocks = 0;
         unsigned numTiles = 0;
-        int persistentCtas = 0;
+        int p2gCtas = 0;
+        int updCtas = 0;
 
         cudaGraphExec_t graph = nullptr;
         unsigned graphVersion = ~0u;

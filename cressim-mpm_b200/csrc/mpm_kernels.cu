@@ -21,6 +21,7 @@
 #include <atomic>
 #include <cmath>
 #include <string>
+#include <type_traits>
 
 #include "mpm_engine.cuh"
 
@@ -29,7 +30,7 @@ namespace crb200
     constexpr unsigned kInvalidKey = 0xFFFFFFFFu;
     constexpr int kTileEdge = 6;
     constexpr int kTileNodes = kTileEdge * kTileEdge * kTileEdge;
-    constexpr int kScanTile = 2048; // blocks per scan tile
+    constexpr int kScanTile = 256; // blocks per scan tile
     constexpr int kScanThreads = 256;
     constexpr int kSortCap = 2048; // particles per block sorted in shared memory
 
@@ -529,7 +530,11 @@ namespace crb200
         }
     }
 
-    // 6. P2G.  Mode 0 MLS (mls_mpm_algorithm.h:147-241), 1 PB (pb_mpm_algorithm.h:150-231),
+}
+#include "p2g_cells.cuh"
+namespace crb200
+{
+    // 6. P2G (per-particle tile atomics; kept for reference timing).  Mode 0 MLS (mls_mpm_algorithm.h:147-241), 1 PB (pb_mpm_algorithm.h:150-231),
     //    2 standard (standard_mpm_algorithm.h:146-215).
     template <int Mode>
     __global__ void __launch_bounds__(128) k_p2g(StepParams p, const SortHeader *__restrict__ hdr,
@@ -783,19 +788,25 @@ namespace crb200
 
     // 8. G2P in particle order.  Mode 0 MLS (mls_mpm_algorithm.h:296-390), 1 PB
     //    (pb_mpm_algorithm.h:286-361, v and C only), 2 standard (standard_mpm_algorithm.h:274-352).
+    //    Node addresses are separable in the block-major layout (addr = AX[i] + AY[j] + AZ[k]); a
+    //    particle whose stencil lies inside the grid skips all per-node bounds tests.  The APIC
+    //    matrix 4/dx sum_n d_r (w v)_c is accumulated as 4/dx dx (sum_n ijk_r (w v)_c - fx_r sum_n (w v)_c).
     template <int Mode>
     __global__ void __launch_bounds__(128) k_g2p(StepParams p, const SortHeader *__restrict__ hdr,
                                                  float4 *__restrict__ xm, float4 *__restrict__ vel,
                                                  const unsigned char *__restrict__ mask, float *__restrict__ F,
                                                  float *__restrict__ Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
-                                                 const float4 *__restrict__ gridV, unsigned *status)
+                                                 const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
+                                                 unsigned *status)
     {
         __shared__ ShapeRec sh[kMaxShapes];
         const GridGeom &g = p.g;
         if (p.numShapes > 0)
+        {
             loadShapes(sh, shapeTable, p.numShapes);
-        __syncthreads();
+            __syncthreads();
+        }
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= p.numActive || !mask[i])
             return;
@@ -807,72 +818,122 @@ namespace crb200
         weights(st.fx, w);
         if (Mode == 2)
             weightGrads(st.fx, dw);
+        const unsigned msk = slicers ? cutMasks[i] : 0u;
         V3 vk = v3(0.f, 0.f, 0.f);
-        if (slicers)
+        if (msk)
         {
             vk = v3(vel[i]);
             if (Mode == 0)
                 vk = vk + v3(p.gravity) * p.dt; // the velocity P2G kicked (mls_mpm_algorithm.h:178)
         }
-        V3 va = v3(0.f, 0.f, 0.f);
-        float Ca[9];
+        V3 S = v3(0.f, 0.f, 0.f);
+        float T[9]; // Modes 0/1: T[3r + c] = sum ijk_r (w v)_c; Mode 2: grad v, column-major
 #pragma unroll
         for (int e = 0; e < 9; ++e)
-            Ca[e] = 0.f;
+            T[e] = 0.f;
+        auto body = [&](int a, int b, int c, float4 gv) {
+            V3 nv = v3(gv);
+            if (Mode != 2 && ((msk >> (a * 9 + b * 3 + c)) & 1u))
+            {
+                const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
+                                ex::mul(ex::sub((float)c, st.fx.z), g.dx));
+                V3 nrm;
+                if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, &nrm))
+                    nv = vk - nrm * dot(vk, nrm) * 2.0f;
+            }
+            const float wt = w[a][0] * w[b][1] * w[c][2];
+            if (Mode == 2)
+            {
+                S = S + nv * wt;
+                const float gw[3] = {dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]};
+                // gradientVelocity += gw.outerProduct(nv): M(r, c) = gw_c * nv_r
+#pragma unroll
+                for (int cc = 0; cc < 3; ++cc)
+                {
+                    T[cc * 3 + 0] += gw[cc] * nv.x;
+                    T[cc * 3 + 1] += gw[cc] * nv.y;
+                    T[cc * 3 + 2] += gw[cc] * nv.z;
+                }
+            }
+            else
+            {
+                const V3 wv = nv * wt;
+                S = S + wv;
+                if (a)
+                {
+                    T[0] += (float)a * wv.x;
+                    T[1] += (float)a * wv.y;
+                    T[2] += (float)a * wv.z;
+                }
+                if (b)
+                {
+                    T[3] += (float)b * wv.x;
+                    T[4] += (float)b * wv.y;
+                    T[5] += (float)b * wv.z;
+                }
+                if (c)
+                {
+                    T[6] += (float)c * wv.x;
+                    T[7] += (float)c * wv.y;
+                    T[8] += (float)c * wv.z;
+                }
+            }
+        };
         if (st.finite)
         {
+            const bool interior = st.b[0] >= 0 && st.b[0] <= g.n.x - 3 && st.b[1] >= 0 && st.b[1] <= g.n.y - 3 &&
+                                  st.b[2] >= 0 && st.b[2] <= g.n.z - 3;
+            if (interior)
+            {
+                unsigned AX[3], AY[3], AZ[3];
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
+                for (int e = 0; e < 3; ++e)
+                {
+                    const int xi = st.b[0] + e, yi = st.b[1] + e, zi = st.b[2] + e;
+                    AX[e] = g.blockBase * 64u + (unsigned)(((xi >> 2) << 6) + (xi & 3));
+                    AY[e] = (unsigned)(((g.nb.x * (yi >> 2)) << 6) + 4 * (yi & 3));
+                    AZ[e] = (unsigned)(((g.nb.x * g.nb.y * (zi >> 2)) << 6) + 16 * (zi & 3));
+                }
 #pragma unroll
-                for (int b = 0; b < 3; ++b)
+                for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                    {
-                        const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
-                        if (!inGrid(g, ni, nj, nk))
-                            continue;
-                        const float4 gv = __ldg(&gridV[nodeAddr(g, ni, nj, nk)]);
-                        V3 nv = v3(gv);
-                        const float wt = w[a][0] * w[b][1] * w[c][2];
-                        if (Mode == 2)
+                    for (int b = 0; b < 3; ++b)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            body(a, b, c, __ldg(&gridV[AX[a] + AY[b] + AZ[c]]));
+            }
+            else
+            {
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        for (int c = 0; c < 3; ++c)
                         {
-                            va = va + nv * wt;
-                            const V3 gw = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2],
-                                             w[a][0] * w[b][1] * dw[c][2]);
-                            // gradientVelocity += gw.outerProduct(nv): M(r, c) = gw_c * nv_r
-#pragma unroll
-                            for (int cc = 0; cc < 3; ++cc)
-#pragma unroll
-                                for (int rr = 0; rr < 3; ++rr)
-                                    Ca[cc * 3 + rr] += comp(gw, cc) * comp(nv, rr);
+                            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                            if (inGrid(g, ni, nj, nk))
+                                body(a, b, c, __ldg(&gridV[nodeAddr(g, ni, nj, nk)]));
                         }
-                        else
-                        {
-                            const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx),
-                                            ex::mul(ex::sub((float)b, st.fx.y), g.dx),
-                                            ex::mul(ex::sub((float)c, st.fx.z), g.dx));
-                            if (slicers)
-                            {
-                                V3 nrm;
-                                if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, &nrm))
-                                    nv = vk - nrm * dot(vk, nrm) * 2.0f;
-                            }
-                            const V3 nw = nv * wt;
-                            va = va + nw;
-                            // outerProduct(nw, d): M(r, c) = nw_c * d_r
-#pragma unroll
-                            for (int cc = 0; cc < 3; ++cc)
-#pragma unroll
-                                for (int rr = 0; rr < 3; ++rr)
-                                    Ca[cc * 3 + rr] += comp(nw, cc) * comp(d, rr);
-                        }
-                    }
+            }
         }
         M3 Cn;
-        const float s4 = 4.f * g.invDx;
+        if (Mode == 2)
+        {
 #pragma unroll
-        for (int e = 0; e < 9; ++e)
-            Cn.m[e] = Mode == 2 ? Ca[e] : Ca[e] * s4;
+            for (int e = 0; e < 9; ++e)
+                Cn.m[e] = T[e];
+        }
+        else
+        {
+            const float s4 = 4.f * g.invDx * g.dx;
+            const float fx[3] = {st.fx.x, st.fx.y, st.fx.z};
+            const float Sv[3] = {S.x, S.y, S.z};
+            // C(r, c) = 4/dx sum d_r (w v)_c, column-major m[3c + r]
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    Cn.m[3 * c + r] = s4 * (T[3 * r + c] - fx[r] * Sv[c]);
+        }
+        const V3 va = S;
         if (Mode == 1)
         {
             vel[i] = make_float4(va.x, va.y, va.z, 0.f);
@@ -1028,10 +1089,16 @@ namespace crb200
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= p.numActive)
             return;
+        if (!(p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER)))
+        {
+            if (i < p.numActive)
+                out[i] = 0u; // no slicer in the scene: nothing is cut
+            return;
+        }
         unsigned msk = 0;
         const V3 x = v3(xm[i]);
         const Stencil st = stencilOf(g, x);
-        if (st.finite && p.numShapes > 0 && p.solverType != CRB200_SOLVER_GPU_STANDARD && mask[i])
+        if (st.finite && p.solverType != CRB200_SOLVER_GPU_STANDARD && mask[i])
         {
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b)
@@ -1179,8 +1246,9 @@ namespace crb200
         int dev = 0, sms = 0, perSm = 0;
         CRB_CHECK(cudaGetDevice(&dev));
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_p2g<0>, 128, 0));
-        persistentCtas = sms * (perSm > 0 ? perSm : 1);
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_p2gCells<0>, 64, 0));
+        p2gCtas = sms * (perSm > 0 ? perSm : 1);
+        updCtas = sms * 8;
         initialized = true;
         configVersion++;
         return CRB200_OK;
@@ -1210,9 +1278,7 @@ namespace crb200
         if (n > 0)
         {
             k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, blockStart, sortPairs);
-            k_blockSort<<<persistentCtas, 256, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds,
-                                                            &header->status);
-            CRB_LAUNCHED(2);
+            CRB_LAUNCHED(1);
         }
         return CRB200_OK;
     }
@@ -1232,6 +1298,11 @@ namespace crb200
             setLastError("step: shapes are enabled but shape ids / shape data / geometry data are not bound");
             return CRB200_ERR_NOT_INITIALIZED;
         }
+        if (numActive > 0 && (!matParams || !matType || !activeMask))
+        {
+            setLastError("step: particle materials or active mask not bound");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
         const StepParams p = params();
         markPhase(0);
         if (numShapes > 0)
@@ -1244,50 +1315,60 @@ namespace crb200
         float4 *cf = reinterpret_cast<float4 *>(shapes.force), *ct = reinterpret_cast<float4 *>(shapes.torque);
         const unsigned stride = (unsigned)numMaxParticles;
         const unsigned pg = (numActive + 127) / 128;
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int updCtas = sms * 8;
         const bool isStd = solverType == CRB200_SOLVER_GPU_STANDARD;
         int r = sortParticles(p, isStd);
         if (r != CRB200_OK)
             return r;
+        // Slicer cut masks of this substep's positions (positions do not change across PB-MPM
+        // iterations, so one evaluation serves every iteration of the step).
+        if (numShapes > 0 && !isStd && pg)
+        {
+            k_cutMasks<<<pg, 128, 0, stream>>>(p, header, positionMass, activeMask, shapeTable, sp, cutMasks);
+            CRB_LAUNCHED(1);
+        }
         markPhase(1);
+        auto p2g = [&](auto mode) -> int {
+            constexpr int M = decltype(mode)::value;
+            k_p2gCells<M><<<p2gCtas, 64, 0, stream>>>(p, header, activeList, blockStart, sortPairs, sortedIds, positionMass,
+                                                       velocity, matParams, matType, F, Cm, V0, stride, cutMasks, gridA,
+                                                       gridF, &header->fp64Fallbacks, &header->status);
+            CRB_LAUNCHED(1);
+            return CRB200_OK;
+        };
+        auto update = [&]() -> int {
+            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
+            CRB_LAUNCHED(1);
+            return CRB200_OK;
+        };
+        auto g2p = [&](auto mode) -> int {
+            constexpr int M = decltype(mode)::value;
+            if (!pg)
+                return CRB200_OK;
+            k_g2p<M><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
+                                             gridV, cutMasks, &header->status);
+            CRB_LAUNCHED(1);
+            return CRB200_OK;
+        };
+        using M0 = std::integral_constant<int, 0>;
+        using M1 = std::integral_constant<int, 1>;
+        using M2 = std::integral_constant<int, 2>;
         if (solverType == CRB200_SOLVER_GPU_MLS)
         {
-            k_p2g<0><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass, velocity,
-                                                         matParams, matType, F, Cm, V0, stride, shapeTable, sp, gridA, gridF,
-                                                         &header->fp64Fallbacks);
+            if ((r = p2g(M0{})) != CRB200_OK) return r;
             markPhase(2);
-            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
-            CRB_LAUNCHED(2);
+            if ((r = update()) != CRB200_OK) return r;
             markPhase(3);
-            if (pg)
-            {
-                k_g2p<0><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
-                                                 gridV, &header->status);
-                CRB_LAUNCHED(1);
-            }
+            if ((r = g2p(M0{})) != CRB200_OK) return r;
         }
         else if (solverType == CRB200_SOLVER_GPU_PB)
         {
             for (int it = 0; it < iterations; ++it)
             {
-                k_p2g<1><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass,
-                                                             velocity, matParams, matType, F, Cm, V0, stride, shapeTable, sp,
-                                                             gridA, gridF, &header->fp64Fallbacks);
-                if (it == 0)
-                    markPhase(2);
-                k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
-                CRB_LAUNCHED(2);
-                if (it == 0)
-                    markPhase(3);
-                if (pg)
-                {
-                    k_g2p<1><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
-                                                     sp, gridV, &header->status);
-                    CRB_LAUNCHED(1);
-                }
+                if ((r = p2g(M1{})) != CRB200_OK) return r;
+                if (it == 0) markPhase(2);
+                if ((r = update()) != CRB200_OK) return r;
+                if (it == 0) markPhase(3);
+                if ((r = g2p(M1{})) != CRB200_OK) return r;
             }
             if (pg)
             {
@@ -1298,26 +1379,13 @@ namespace crb200
         }
         else
         {
-            k_p2g<2><<<persistentCtas, 128, 0, stream>>>(p, header, activeList, blockStart, sortedIds, positionMass, velocity,
-                                                         matParams, matType, F, Cm, V0, stride, shapeTable, sp, gridA, gridF,
-                                                         &header->fp64Fallbacks);
+            if ((r = p2g(M2{})) != CRB200_OK) return r;
             markPhase(2);
-            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
-            CRB_LAUNCHED(2);
+            if ((r = update()) != CRB200_OK) return r;
             markPhase(3);
-            if (pg)
-            {
-                k_g2p<2><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
-                                                 gridV, &header->status);
-                CRB_LAUNCHED(1);
-            }
+            if ((r = g2p(M2{})) != CRB200_OK) return r;
         }
         markPhase(4);
-        if (keepCutMasks && pg)
-        {
-            k_cutMasks<<<pg, 128, 0, stream>>>(p, header, positionMass, activeMask, shapeTable, sp, cutMasks);
-            CRB_LAUNCHED(1);
-        }
         if (phaseTiming)
             return collectPhaseTimes();
         return CRB200_OK;

@@ -1,0 +1,439 @@
+// P2G with one thread per grid cell (included by mpm_kernels.cu).
+//
+// One 64-thread CTA takes one 4x4x4-cell block of the sorted particle list:
+//   1. counting sort of the block's (cell, id) pairs by cell in shared memory, then insertion sort
+//      by id inside each cell: this is the canonical order (cell key, particle id), written back
+//      to sortedIds;
+//   2. the block's particles are staged 128 at a time: per particle 16 floats (the affine
+//      contribution u + i*a0 + j*a1 + k*a2 of MLS / PB-MPM, mass, fractional position);
+//   3. thread c accumulates the 27 stencil nodes of cell c in registers over all particles of
+//      its cell (in id order, so the sums inside a block are deterministic);
+//   4. a 27-phase flush adds the registers into a per-warp shared-memory 6x6x6 node tile: in one
+//      phase the 32 lanes of a warp write 32 distinct nodes, so no atomics are needed;
+//   5. the two warp tiles are summed in a fixed order and each touched node gets one float4
+//      vector atomic in the block-major accumulation grid.
+// Particles whose stencil base lies outside the grid, and blocks holding more than kCellCap
+// particles, take a per-particle path with global vector atomics instead.
+#pragma once
+
+namespace crb200
+{
+    constexpr int kCellCap = 1024; // particles of one block sorted in shared memory
+    constexpr int kChunk = 128;    // particles staged at once
+    constexpr int kRec = 16;       // floats per staged particle
+
+    // Per-particle scatter with global vector atomics (outliers and oversized blocks).
+    // Mode 0 MLS, 1 PB (u/a already include the mass), 2 standard momentum, 3 standard force.
+    template <int Mode>
+    __device__ __forceinline__ void scatterGlobal(const StepParams &p, const Stencil &st, const float *rec,
+                                                  unsigned cutMask, float4 *__restrict__ gridA, float4 *__restrict__ gridF)
+    {
+        const GridGeom &g = p.g;
+        float w[3][3], dw[3][3];
+        weights(st.fx, w);
+        if (Mode == 3)
+            weightGrads(st.fx, dw);
+        const V3 u = v3(rec[0], rec[1], rec[2]);
+        const float m = rec[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    const int ni = st.b[0] + i, nj = st.b[1] + j, nk = st.b[2] + k;
+                    if (!inGrid(g, ni, nj, nk) || ((cutMask >> (i * 9 + j * 3 + k)) & 1u))
+                        continue;
+                    const float wt = w[i][0] * w[j][1] * w[k][2];
+                    const unsigned a = nodeAddr(g, ni, nj, nk);
+                    if (Mode == 3)
+                    {
+                        const V3 gw = v3(dw[i][0] * w[j][1] * w[k][2], w[i][0] * dw[j][1] * w[k][2],
+                                         w[i][0] * w[j][1] * dw[k][2]);
+                        const float wm = wt * m;
+                        const V3 f = v3(p.gravity.x * wm + rec[4] * gw.x + rec[7] * gw.y + rec[10] * gw.z,
+                                        p.gravity.y * wm + rec[5] * gw.x + rec[8] * gw.y + rec[11] * gw.z,
+                                        p.gravity.z * wm + rec[6] * gw.x + rec[9] * gw.y + rec[12] * gw.z);
+                        atomicAdd(&gridF[a], make_float4(f.x, f.y, f.z, 0.f));
+                    }
+                    else
+                    {
+                        V3 val = u;
+                        if (Mode <= 1)
+                            val = u + v3(rec[4], rec[5], rec[6]) * (float)i + v3(rec[7], rec[8], rec[9]) * (float)j +
+                                  v3(rec[10], rec[11], rec[12]) * (float)k;
+                        atomicAdd(&gridA[a], make_float4(val.x * wt, val.y * wt, val.z * wt, m * wt));
+                    }
+                }
+    }
+
+    // Build the staged record of one particle.  Record layout:
+    //   [0..2] u, [3] m, [4..12] a0 a1 a2 (MLS / PB) or -V0*tau column-major (standard force),
+    //   [13..15] fx.
+    // Returns false when the particle must not go through the cell path (non-finite position or a
+    // stencil base outside [0, n-2]); such particles are scattered here with global atomics.
+    template <int Mode>
+    __device__ __forceinline__ bool stageParticle(const StepParams &p, unsigned id, const float4 *__restrict__ xm,
+                                                  const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
+                                                  const int *__restrict__ matType, const float *__restrict__ F,
+                                                  float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
+                                                  unsigned cutMask, bool scatterOutliers, float4 *__restrict__ gridA,
+                                                  float4 *__restrict__ gridF, unsigned *fp64Count, float rec[kRec])
+    {
+        const GridGeom &g = p.g;
+        const float4 x4 = xm[id];
+        const Stencil st = stencilOf(g, v3(x4));
+        const float m = x4.w;
+#pragma unroll
+        for (int e = 0; e < kRec; ++e)
+            rec[e] = 0.f;
+        if (!st.finite)
+            return false;
+        const V3 v = v3(vel[id]);
+        M3 Fp;
+        loadM3(F, stride, id, Fp);
+        const float dx = g.dx;
+        if (Mode == 0 || Mode == 1)
+        {
+            M3 A;
+            V3 base;
+            if (Mode == 0)
+            {
+                M3 Cp;
+                loadM3(Cm, stride, id, Cp);
+                const float4 mp = matParams[id];
+                const M3 s = kirchhoffStress(Fp, mp.x, mp.y, matType[id]);
+                const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[id];
+#pragma unroll
+                for (int e = 0; e < 9; ++e)
+                    A.m[e] = s.m[e] * coef + Cp.m[e] * m;
+                base = (v + v3(p.gravity) * p.dt) * m;
+            }
+            else
+            {
+                M3 Cp;
+                loadM3(Cm, stride, id, Cp);
+                const float4 mp = matParams[id];
+                const int mt = matType[id];
+                if (mt == 1 || mt == 0)
+                {
+                    // solveMaterialConstraints (constitutive_models.h:123-156)
+                    M3 tF;
+#pragma unroll
+                    for (int e = 0; e < 9; ++e)
+                        tF.m[e] = Cp.m[e] * p.dt + ((e % 4) == 0 ? 1.f : 0.f);
+                    tF = matmul(tF, Fp);
+                    const M3 R = pbRotationTarget(tF, fp64Count);
+                    const float detF = det3(tF);
+                    const float cd = fminf(fmaxf(fabsf(detF), 0.1f), 1000.0f);
+                    const float qs = 1.0f / (copysignf(1.0f, detF) * sqrtf(cd));
+                    M3 tgt;
+#pragma unroll
+                    for (int e = 0; e < 9; ++e)
+                        tgt.m[e] = R.m[e] * mp.y + (tF.m[e] * qs) * (1.0f - mp.y);
+                    const M3 TF = matmul(tgt, inverse3(Fp));
+#pragma unroll
+                    for (int e = 0; e < 9; ++e)
+                        Cp.m[e] = Cp.m[e] + ((TF.m[e] - ((e % 4) == 0 ? 1.f : 0.f)) - Cp.m[e] * p.dt) * mp.x;
+                    storeM3(Cm, stride, id, Cp);
+                }
+#pragma unroll
+                for (int e = 0; e < 9; ++e)
+                    A.m[e] = Cp.m[e] * m;
+                base = v * m;
+            }
+            // u = base - A (fx dx); a_c = dx * A column c
+            const V3 fd = v3(st.fx.x * dx, st.fx.y * dx, st.fx.z * dx);
+            rec[0] = base.x - (A.m[0] * fd.x + A.m[3] * fd.y + A.m[6] * fd.z);
+            rec[1] = base.y - (A.m[1] * fd.x + A.m[4] * fd.y + A.m[7] * fd.z);
+            rec[2] = base.z - (A.m[2] * fd.x + A.m[5] * fd.y + A.m[8] * fd.z);
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+                rec[4 + e] = A.m[e] * dx;
+        }
+        else
+        {
+            // standard MPM: momentum v m, force -V0 tau grad w + g w m (standard_mpm_algorithm.h:166-206)
+            const float4 mp = matParams[id];
+            const M3 s = kirchhoffStress(Fp, mp.x, mp.y, matType[id]);
+            const float nv0 = -V0[id];
+            rec[0] = v.x * m;
+            rec[1] = v.y * m;
+            rec[2] = v.z * m;
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+                rec[4 + e] = s.m[e] * nv0;
+        }
+        rec[3] = m;
+        rec[13] = st.fx.x;
+        rec[14] = st.fx.y;
+        rec[15] = st.fx.z;
+        const bool inside = st.b[0] >= 0 && st.b[0] <= g.n.x - 2 && st.b[1] >= 0 && st.b[1] <= g.n.y - 2 &&
+                            st.b[2] >= 0 && st.b[2] <= g.n.z - 2;
+        if (!inside)
+        {
+            if (!scatterOutliers)
+                return false;
+            if (Mode == 2)
+            {
+                scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
+                scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
+            }
+            else
+                scatterGlobal<Mode>(p, st, rec, cutMask, gridA, gridF);
+            return false;
+        }
+        return true;
+    }
+
+    template <int Mode>
+    __global__ void __launch_bounds__(64) k_p2gCells(StepParams p, const SortHeader *__restrict__ hdr,
+                                                     const unsigned *__restrict__ activeList,
+                                                     const unsigned *__restrict__ blockStart,
+                                                     const unsigned long long *__restrict__ pairs,
+                                                     unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
+                                                     const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
+                                                     const int *__restrict__ matType, const float *__restrict__ F,
+                                                     float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
+                                                     const unsigned *__restrict__ cutMasks, float4 *__restrict__ gridA,
+                                                     float4 *__restrict__ gridF, unsigned *fp64Count, unsigned *status)
+    {
+        __shared__ unsigned sIds[kCellCap];
+        __shared__ unsigned sTmp[kCellCap];
+        __shared__ unsigned char sCell[kCellCap];
+        __shared__ unsigned short sRank[kCellCap];
+        __shared__ unsigned sCnt[64];
+        __shared__ unsigned sStart[65];
+        __shared__ unsigned sWarpTot;
+        __shared__ float sRec[kRec * kChunk];
+        __shared__ unsigned sMask[kChunk];
+        __shared__ float sTile[2][4 * kTileNodes];
+
+        const GridGeom &g = p.g;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const int passes = Mode == 2 ? 2 : 1;
+        for (int t = tid; t < 2 * 4 * kTileNodes; t += 64)
+            (&sTile[0][0])[t] = 0.f;
+        __syncthreads();
+        const unsigned nAct = hdr->numActiveBlocks;
+        const int cx = tid & 3, cy = (tid >> 2) & 3, cz = tid >> 4;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
+            if (cnt > (unsigned)kCellCap)
+            {
+                // oversized block: canonical order by rank counting, then per-particle global atomics
+                if (tid == 0)
+                    atomicOr(status, CRB200_STATUS_BLOCK_OVERFLOW);
+                for (unsigned t = tid; t < cnt; t += 64)
+                {
+                    const unsigned long long e = pairs[start + t];
+                    unsigned rank = 0;
+                    for (unsigned u2 = 0; u2 < cnt; ++u2)
+                        rank += pairs[start + u2] < e;
+                    sortedIds[start + rank] = (unsigned)e;
+                    const unsigned id = (unsigned)e;
+                    float rec[kRec];
+                    const unsigned msk = slicers ? cutMasks[id] : 0u;
+                    if (stageParticle<Mode>(p, id, xm, vel, matParams, matType, F, Cm, V0, stride, msk, true, gridA,
+                                            gridF, fp64Count, rec))
+                    {
+                        const Stencil st = stencilOf(g, v3(xm[id]));
+                        if (Mode == 2)
+                        {
+                            scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
+                            scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
+                        }
+                        else
+                            scatterGlobal<Mode>(p, st, rec, msk, gridA, gridF);
+                    }
+                }
+                continue;
+            }
+            // 1. counting sort by cell, then by id inside each cell
+            sCnt[tid] = 0;
+            __syncthreads();
+            for (unsigned t = tid; t < cnt; t += 64)
+            {
+                const unsigned long long pr = pairs[start + t];
+                const unsigned c = (unsigned)(pr >> 32);
+                sCell[t] = (unsigned char)c;
+                sTmp[t] = (unsigned)pr;
+                sRank[t] = (unsigned short)atomicAdd(&sCnt[c], 1u);
+            }
+            __syncthreads();
+            {
+                const unsigned v = sCnt[tid];
+                unsigned inc = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o)
+                        inc += y;
+                }
+                if (tid == 31)
+                    sWarpTot = inc;
+                __syncthreads();
+                const unsigned excl = inc - v + (warp ? sWarpTot : 0u);
+                sStart[tid] = excl;
+                if (tid == 63)
+                    sStart[64] = excl + v;
+            }
+            __syncthreads();
+            for (unsigned t = tid; t < cnt; t += 64)
+                sIds[sStart[sCell[t]] + sRank[t]] = sTmp[t];
+            __syncthreads();
+            const unsigned cs = sStart[tid], ce = sStart[tid + 1];
+            for (unsigned a = cs + 1; a < ce; ++a)
+            {
+                const unsigned key = sIds[a];
+                unsigned j = a;
+                while (j > cs && sIds[j - 1] > key)
+                {
+                    sIds[j] = sIds[j - 1];
+                    --j;
+                }
+                sIds[j] = key;
+            }
+            __syncthreads();
+            for (unsigned t = tid; t < cnt; t += 64)
+                sortedIds[start + t] = sIds[t];
+
+            for (int pass = 0; pass < passes; ++pass)
+            {
+                // 2./3. stage and accumulate
+                float acc[27][4];
+#pragma unroll
+                for (int n = 0; n < 27; ++n)
+                {
+                    acc[n][0] = 0.f;
+                    acc[n][1] = 0.f;
+                    acc[n][2] = 0.f;
+                    acc[n][3] = 0.f;
+                }
+                for (unsigned c0 = 0; c0 < cnt; c0 += kChunk)
+                {
+                    for (unsigned t = tid; t < (unsigned)kChunk && c0 + t < cnt; t += 64)
+                    {
+                        const unsigned id = sIds[c0 + t];
+                        const unsigned msk = slicers ? cutMasks[id] : 0u;
+                        float rec[kRec];
+                        // outliers are scattered once, in the first pass, with global atomics
+                        const bool ok = stageParticle<Mode>(p, id, xm, vel, matParams, matType, F, Cm, V0, stride, msk,
+                                                            pass == 0, gridA, gridF, fp64Count, rec);
+                        if (!ok)
+                        {
+#pragma unroll
+                            for (int e = 0; e < kRec; ++e)
+                                rec[e] = 0.f;
+                        }
+#pragma unroll
+                        for (int e = 0; e < kRec; ++e)
+                            sRec[e * kChunk + t] = rec[e];
+                        sMask[t] = msk;
+                    }
+                    __syncthreads();
+                    const unsigned lo = max(cs, c0), hi = min(ce, c0 + (unsigned)kChunk);
+                    for (unsigned q = lo; q < hi; ++q)
+                    {
+                        const unsigned r = q - c0;
+                        const V3 u = v3(sRec[0 * kChunk + r], sRec[1 * kChunk + r], sRec[2 * kChunk + r]);
+                        const float m = sRec[3 * kChunk + r];
+                        const V3 a0 = v3(sRec[4 * kChunk + r], sRec[5 * kChunk + r], sRec[6 * kChunk + r]);
+                        const V3 a1 = v3(sRec[7 * kChunk + r], sRec[8 * kChunk + r], sRec[9 * kChunk + r]);
+                        const V3 a2 = v3(sRec[10 * kChunk + r], sRec[11 * kChunk + r], sRec[12 * kChunk + r]);
+                        const V3 fx = v3(sRec[13 * kChunk + r], sRec[14 * kChunk + r], sRec[15 * kChunk + r]);
+                        const unsigned msk = slicers ? sMask[r] : 0u;
+                        float w[3][3], dw[3][3];
+                        weights(fx, w);
+                        if (Mode == 2 && pass == 1)
+                            weightGrads(fx, dw);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                                for (int k = 0; k < 3; ++k)
+                                {
+                                    const int n = i * 9 + j * 3 + k;
+                                    if (slicers && ((msk >> n) & 1u))
+                                        continue;
+                                    const float wt = w[i][0] * w[j][1] * w[k][2];
+                                    if (Mode == 2 && pass == 1)
+                                    {
+                                        const float wm = wt * m;
+                                        const float gx = dw[i][0] * w[j][1] * w[k][2], gy = w[i][0] * dw[j][1] * w[k][2],
+                                                    gz = w[i][0] * w[j][1] * dw[k][2];
+                                        acc[n][0] += p.gravity.x * wm + a0.x * gx + a1.x * gy + a2.x * gz;
+                                        acc[n][1] += p.gravity.y * wm + a0.y * gx + a1.y * gy + a2.y * gz;
+                                        acc[n][2] += p.gravity.z * wm + a0.z * gx + a1.z * gy + a2.z * gz;
+                                    }
+                                    else
+                                    {
+                                        V3 val = u;
+                                        if (Mode <= 1)
+                                            val = u + a0 * (float)i + a1 * (float)j + a2 * (float)k;
+                                        acc[n][0] += val.x * wt;
+                                        acc[n][1] += val.y * wt;
+                                        acc[n][2] += val.z * wt;
+                                        acc[n][3] += m * wt;
+                                    }
+                                }
+                    }
+                    __syncthreads();
+                }
+                // 4. phased flush of the registers into this warp's tile
+                float *tile = sTile[warp];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                        {
+                            const int n = i * 9 + j * 3 + k;
+                            const int t = (cx + i) + kTileEdge * ((cy + j) + kTileEdge * (cz + k));
+                            tile[t] += acc[n][3];
+                            tile[kTileNodes + t] += acc[n][0];
+                            tile[2 * kTileNodes + t] += acc[n][1];
+                            tile[3 * kTileNodes + t] += acc[n][2];
+                            __syncwarp();
+                        }
+                __syncthreads();
+                // 5. fixed-order sum of the warp tiles, one vector atomic per touched node
+                for (int t = tid; t < kTileNodes; t += 64)
+                {
+                    const float m = sTile[0][t] + sTile[1][t];
+                    const float px = sTile[0][kTileNodes + t] + sTile[1][kTileNodes + t];
+                    const float py = sTile[0][2 * kTileNodes + t] + sTile[1][2 * kTileNodes + t];
+                    const float pz = sTile[0][3 * kTileNodes + t] + sTile[1][3 * kTileNodes + t];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                    {
+                        sTile[0][c * kTileNodes + t] = 0.f;
+                        sTile[1][c * kTileNodes + t] = 0.f;
+                    }
+                    const int tx = t % kTileEdge, ty = (t / kTileEdge) % kTileEdge, tz = t / (kTileEdge * kTileEdge);
+                    const int i = 4 * bx + tx, j = 4 * by + ty, k = 4 * bz + tz;
+                    if (!inGrid(g, i, j, k))
+                        continue;
+                    const unsigned a = nodeAddr(g, i, j, k);
+                    if (Mode == 2 && pass == 1)
+                    {
+                        if (px != 0.f || py != 0.f || pz != 0.f)
+                            atomicAdd(&gridF[a], make_float4(px, py, pz, 0.f));
+                    }
+                    else if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f)
+                        atomicAdd(&gridA[a], make_float4(px, py, pz, m));
+                }
+                __syncthreads();
+            }
+        }
+    }
+} // namespace crb200

@@ -241,8 +241,9 @@ CRB200_API int CrB200SolverCopySortState(CrB200SolverHandle solver, unsigned int
                                          unsigned int *sortedIds, unsigned int *outNumSortedHost);
 
 /* Slicer cut masks of the most recent substep (bit i*9 + j*3 + k set when particle and stencil
- * node (i, j, k) lie on different sides of a slicer; mls_mpm_algorithm.h:200-210).  Device
- * buffer of numMaxParticles uint32.  Fails with CRB200_ERR_UNSUPPORTED unless cut masks are on. */
+ * node (i, j, k) lie on different sides of a slicer; mls_mpm_algorithm.h:200-210), evaluated on
+ * the positions the substep started from.  Device buffer of numActive uint32; all zero when the
+ * scene has no slicer shape. */
 CRB200_API int CrB200SolverCopyCutMasks(CrB200SolverHandle solver, unsigned int *masks);
 
 /* Sticky device status word (CRB200_STATUS_*), read with a bounded wait of timeoutMs
@@ -251,11 +252,8 @@ CRB200_API int CrB200SolverGetStatus(CrB200SolverHandle solver, unsigned int *ou
                                      int timeoutMs);
 CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
 
-/* Option switches: CRB200_OPT_DETERMINISTIC orders every floating-point reduction so that two
- * runs on identical inputs give bitwise-identical outputs; CRB200_OPT_CUT_MASKS keeps the
- * per-particle slicer masks for CrB200SolverCopyCutMasks. */
-#define CRB200_OPT_DETERMINISTIC 1
-#define CRB200_OPT_CUT_MASKS 2
+/* Option switches: CRB200_OPT_PHASE_TIMING records CUDA events around the phases of every
+ * substep (see CrB200SolverGetPhaseTimes); it disables CUDA-graph replay while on. */
 #define CRB200_OPT_PHASE_TIMING 3
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
