@@ -32,9 +32,11 @@ namespace crb200
     };
 
     // One rigid shape of a scene, gathered once per substep from the bound struct-of-arrays.
+    // cull.x / cull.y: a node / particle whose local SDF lower bound (sdfLowerBound) is at least
+    // this value cannot be in contact with the shape (+inf disables the test).
     struct __align__(16) ShapeRec
     {
-        float4 pos, rot, invScale, linVel, angVel, params0, gparams, comInvMass, inertia0, inertia1;
+        float4 pos, rot, invScale, linVel, angVel, params0, gparams, comInvMass, inertia0, inertia1, cull;
         int kind, gtype, id, pad;
     };
 
@@ -238,7 +240,7 @@ namespace crb200
         return acc;
     }
 
-    static __device__ __noinline__ bool geometrySdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, V3 &grad, float &dist,
+    static __device__ __forceinline__ bool geometrySdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, V3 &grad, float &dist,
                                              V3 &tangent)
     {
         bool inSpine = false;
@@ -416,6 +418,27 @@ namespace crb200
         return inSpine;
     }
 
+    // Conservative lower bound of the local SDF of the analytic geometries (box, sphere, plane,
+    // capsule; sdf.h:77-150).  For a unit-gradient SDF the scaled distance is at least
+    // bound / max(invScale), so a point whose bound reaches (smooth + fatten) * max(invScale) is
+    // outside the contact band and the full evaluation can be skipped.
+    __device__ __forceinline__ float sdfLowerBound(V3 lp, int gtype, const float4 &p0)
+    {
+        switch (gtype)
+        {
+        case G_BOX:
+            return fmaxf(fabsf(lp.x) - p0.x, fmaxf(fabsf(lp.y) - p0.y, fabsf(lp.z) - p0.z));
+        case G_SPHERE:
+            return sqrtf(sq(lp)) - p0.x;
+        case G_PLANE:
+            return lp.y;
+        case G_CAPSULE:
+            return fmaxf(sqrtf(lp.x * lp.x + lp.z * lp.z), fabsf(lp.y) - p0.y) - p0.x;
+        default:
+            return -kMaxF32;
+        }
+    }
+
     // resolveRigidCollision (mpm_rigid_contact.h:101-399).
     //   isParticle = false: grid node with velocity vel (mass m) evaluated at pos; contact inside
     //       the smooth distance, separating nodes skipped, Coulomb-like friction, drag, rigid
@@ -433,6 +456,9 @@ namespace crb200
             const V3 isc = v3(r.invScale);
             const V3 wrel = pos - v3(r.pos);
             const V3 lp = mul(qrotInv(r.rot, wrel), isc);
+            const float cull = IsParticle ? r.cull.y : r.cull.x;
+            if (cull < kMaxF32 && sdfLowerBound(lp, r.gtype, r.gparams) >= cull)
+                continue;
             V3 grad, tangent = v3(0.f, 0.f, 0.f);
             float dist;
             const bool onSpine = geometrySdf(lp, r.gtype, r.gparams, sdf, grad, dist, tangent);

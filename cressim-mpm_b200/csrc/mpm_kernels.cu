@@ -165,6 +165,16 @@ namespace crb200
             r.gtype = ge.type[gid];
             r.id = id;
             r.pad = 0;
+            {
+                // culling thresholds (sdfLowerBound), with a small safety margin
+                const float maxIsc = fmaxf(fabsf(r.invScale.x), fmaxf(fabsf(r.invScale.y), fabsf(r.invScale.z)));
+                const bool analytic = r.gtype == G_BOX || r.gtype == G_SPHERE || r.gtype == G_PLANE || r.gtype == G_CAPSULE;
+                const float band = r.params0.x + r.params0.w, pband = r.params0.w;
+                r.cull.x = (analytic && band >= 0.f && isfinite(band * maxIsc)) ? band * maxIsc * 1.0001f + 1e-6f : kMaxF32;
+                r.cull.y = (analytic && pband >= 0.f && isfinite(pband * maxIsc)) ? pband * maxIsc * 1.0001f + 1e-6f : kMaxF32;
+                r.cull.z = 0.f;
+                r.cull.w = 0.f;
+            }
             out[s] = r;
             int f = 0;
             if (r.gtype == G_QUAD_SLICER || r.gtype == G_TRIMESH_SLICER)
@@ -904,8 +914,11 @@ namespace crb200
             }
             else
             {
+#pragma unroll
                 for (int a = 0; a < 3; ++a)
+#pragma unroll
                     for (int b = 0; b < 3; ++b)
+#pragma unroll
                         for (int c = 0; c < 3; ++c)
                         {
                             const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;

@@ -4,13 +4,12 @@
 //   1. counting sort of the block's (cell, id) pairs by cell in shared memory, then insertion sort
 //      by id inside each cell: this is the canonical order (cell key, particle id), written back
 //      to sortedIds;
-//   2. the block's particles are staged 128 at a time: per particle 16 floats (the affine
-//      contribution u + i*a0 + j*a1 + k*a2 of MLS / PB-MPM, mass, fractional position);
-//   3. thread c accumulates the 27 stencil nodes of cell c in registers over all particles of
-//      its cell (in id order, so the sums inside a block are deterministic);
-//   4. a 27-phase flush adds the registers into a per-warp shared-memory 6x6x6 node tile: in one
+//   2. thread c walks the particles of cell c in id order, loading each one a particle ahead,
+//      turns it into the affine contribution u + i*a0 + j*a1 + k*a2 (MLS / PB-MPM) and
+//      accumulates the 27 stencil nodes in registers (the sums inside a block are deterministic);
+//   3. a 27-phase flush adds the registers into a per-warp shared-memory 6x6x6 node tile: in one
 //      phase the 32 lanes of a warp write 32 distinct nodes, so no atomics are needed;
-//   5. the two warp tiles are summed in a fixed order and each touched node gets one float4
+//   4. the two warp tiles are summed in a fixed order and each touched node gets one float4
 //      vector atomic in the block-major accumulation grid.
 // Particles whose stencil base lies outside the grid, and blocks holding more than kCellCap
 // particles, take a per-particle path with global vector atomics instead.
@@ -19,8 +18,9 @@
 namespace crb200
 {
     constexpr int kCellCap = 1024; // particles of one block sorted in shared memory
-    constexpr int kChunk = 128;    // particles staged at once
     constexpr int kRec = 16;       // floats per staged particle
+    constexpr int kCellRun = 9;    // particles a cell thread accumulates; the rest of a cell's
+                                   // particles go through per-particle vector atomics
 
     // Per-particle scatter with global vector atomics (outliers and oversized blocks).
     // Mode 0 MLS, 1 PB (u/a already include the mass), 2 standard momentum, 3 standard force.
@@ -68,43 +68,74 @@ namespace crb200
                 }
     }
 
-    // Build the staged record of one particle.  Record layout:
+    // Raw particle data a P2G thread needs (loaded one particle ahead of its use).
+    struct RawParticle
+    {
+        float4 x4, v4, mp;
+        float F[9], C[9];
+        float v0;
+        int mt;
+    };
+
+    template <int Mode>
+    __device__ __forceinline__ void loadRaw(unsigned id, const float4 *__restrict__ xm, const float4 *__restrict__ vel,
+                                            const float4 *__restrict__ matParams, const int *__restrict__ matType,
+                                            const float *__restrict__ F, const float *__restrict__ Cm,
+                                            const float *__restrict__ V0, unsigned stride, RawParticle &r)
+    {
+        r.x4 = xm[id];
+        r.v4 = vel[id];
+        r.mp = matParams[id];
+        r.mt = matType[id];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            r.F[k] = F[k * stride + id];
+        if (Mode != 2)
+        {
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                r.C[k] = Cm[k * stride + id];
+        }
+        r.v0 = (Mode == 1) ? 0.f : V0[id];
+    }
+
+    // Record of one particle for the cell accumulation:
     //   [0..2] u, [3] m, [4..12] a0 a1 a2 (MLS / PB) or -V0*tau column-major (standard force),
     //   [13..15] fx.
     // Returns false when the particle must not go through the cell path (non-finite position or a
-    // stencil base outside [0, n-2]); such particles are scattered here with global atomics.
+    // stencil base outside [0, n-2]); such particles are scattered here with global atomics when
+    // scatterOutliers is set.
     template <int Mode>
-    __device__ __forceinline__ bool stageParticle(const StepParams &p, unsigned id, const float4 *__restrict__ xm,
-                                                  const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
-                                                  const int *__restrict__ matType, const float *__restrict__ F,
-                                                  float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
-                                                  unsigned cutMask, bool scatterOutliers, float4 *__restrict__ gridA,
-                                                  float4 *__restrict__ gridF, unsigned *fp64Count, float rec[kRec])
+    __device__ __forceinline__ bool buildRecord(const StepParams &p, unsigned id, const RawParticle &raw,
+                                                float *__restrict__ Cm, unsigned stride, unsigned cutMask,
+                                                bool scatterOutliers, float4 *__restrict__ gridA,
+                                                float4 *__restrict__ gridF, unsigned *fp64Count, float rec[kRec])
     {
         const GridGeom &g = p.g;
-        const float4 x4 = xm[id];
-        const Stencil st = stencilOf(g, v3(x4));
-        const float m = x4.w;
+        const Stencil st = stencilOf(g, v3(raw.x4));
+        const float m = raw.x4.w;
 #pragma unroll
         for (int e = 0; e < kRec; ++e)
             rec[e] = 0.f;
         if (!st.finite)
             return false;
-        const V3 v = v3(vel[id]);
+        const V3 v = v3(raw.v4);
         M3 Fp;
-        loadM3(F, stride, id, Fp);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            Fp.m[e] = raw.F[e];
         const float dx = g.dx;
         if (Mode == 0 || Mode == 1)
         {
-            M3 A;
+            M3 A, Cp;
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+                Cp.m[e] = raw.C[e];
             V3 base;
             if (Mode == 0)
             {
-                M3 Cp;
-                loadM3(Cm, stride, id, Cp);
-                const float4 mp = matParams[id];
-                const M3 s = kirchhoffStress(Fp, mp.x, mp.y, matType[id]);
-                const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[id];
+                const M3 s = kirchhoffStress(Fp, raw.mp.x, raw.mp.y, raw.mt);
+                const float coef = -p.dt * 4.f * g.invDx * g.invDx * raw.v0;
 #pragma unroll
                 for (int e = 0; e < 9; ++e)
                     A.m[e] = s.m[e] * coef + Cp.m[e] * m;
@@ -112,11 +143,7 @@ namespace crb200
             }
             else
             {
-                M3 Cp;
-                loadM3(Cm, stride, id, Cp);
-                const float4 mp = matParams[id];
-                const int mt = matType[id];
-                if (mt == 1 || mt == 0)
+                if (raw.mt == 1 || raw.mt == 0)
                 {
                     // solveMaterialConstraints (constitutive_models.h:123-156)
                     M3 tF;
@@ -131,11 +158,11 @@ namespace crb200
                     M3 tgt;
 #pragma unroll
                     for (int e = 0; e < 9; ++e)
-                        tgt.m[e] = R.m[e] * mp.y + (tF.m[e] * qs) * (1.0f - mp.y);
+                        tgt.m[e] = R.m[e] * raw.mp.y + (tF.m[e] * qs) * (1.0f - raw.mp.y);
                     const M3 TF = matmul(tgt, inverse3(Fp));
 #pragma unroll
                     for (int e = 0; e < 9; ++e)
-                        Cp.m[e] = Cp.m[e] + ((TF.m[e] - ((e % 4) == 0 ? 1.f : 0.f)) - Cp.m[e] * p.dt) * mp.x;
+                        Cp.m[e] = Cp.m[e] + ((TF.m[e] - ((e % 4) == 0 ? 1.f : 0.f)) - Cp.m[e] * p.dt) * raw.mp.x;
                     storeM3(Cm, stride, id, Cp);
                 }
 #pragma unroll
@@ -155,9 +182,8 @@ namespace crb200
         else
         {
             // standard MPM: momentum v m, force -V0 tau grad w + g w m (standard_mpm_algorithm.h:166-206)
-            const float4 mp = matParams[id];
-            const M3 s = kirchhoffStress(Fp, mp.x, mp.y, matType[id]);
-            const float nv0 = -V0[id];
+            const M3 s = kirchhoffStress(Fp, raw.mp.x, raw.mp.y, raw.mt);
+            const float nv0 = -raw.v0;
             rec[0] = v.x * m;
             rec[1] = v.y * m;
             rec[2] = v.z * m;
@@ -187,6 +213,66 @@ namespace crb200
         return true;
     }
 
+    // Adds one particle's 27 node contributions to the cell thread's registers.
+    template <int Mode, bool Masked>
+    __device__ __forceinline__ void accumulateCell(const StepParams &p, const float rec[kRec], unsigned msk, int pass,
+                                                   float acc[27][4])
+    {
+        const V3 u = v3(rec[0], rec[1], rec[2]);
+        const float m = rec[3];
+        const V3 a0 = v3(rec[4], rec[5], rec[6]);
+        const V3 a1 = v3(rec[7], rec[8], rec[9]);
+        const V3 a2 = v3(rec[10], rec[11], rec[12]);
+        const V3 fx = v3(rec[13], rec[14], rec[15]);
+        float w[3][3], dw[3][3];
+        weights(fx, w);
+        if (Mode == 2 && pass == 1)
+            weightGrads(fx, dw);
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+        {
+            const V3 ui = u + a0 * (float)i;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+            {
+                const V3 uij = ui + a1 * (float)j;
+                const float wij = w[i][0] * w[j][1];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    const int n = i * 9 + j * 3 + k;
+                    if (Masked && ((msk >> n) & 1u))
+                        continue;
+                    const float wt = wij * w[k][2];
+                    if (Mode == 2 && pass == 1)
+                    {
+                        const float wm = wt * m;
+                        const float gx = dw[i][0] * w[j][1] * w[k][2], gy = w[i][0] * dw[j][1] * w[k][2],
+                                    gz = wij * dw[k][2];
+                        acc[n][0] += p.gravity.x * wm + a0.x * gx + a1.x * gy + a2.x * gz;
+                        acc[n][1] += p.gravity.y * wm + a0.y * gx + a1.y * gy + a2.y * gz;
+                        acc[n][2] += p.gravity.z * wm + a0.z * gx + a1.z * gy + a2.z * gz;
+                    }
+                    else if (Mode == 2)
+                    {
+                        acc[n][0] += u.x * wt;
+                        acc[n][1] += u.y * wt;
+                        acc[n][2] += u.z * wt;
+                        acc[n][3] += m * wt;
+                    }
+                    else
+                    {
+                        const V3 val = uij + a2 * (float)k;
+                        acc[n][0] += val.x * wt;
+                        acc[n][1] += val.y * wt;
+                        acc[n][2] += val.z * wt;
+                        acc[n][3] += m * wt;
+                    }
+                }
+            }
+        }
+    }
+
     template <int Mode>
     __global__ void __launch_bounds__(64) k_p2gCells(StepParams p, const SortHeader *__restrict__ hdr,
                                                      const unsigned *__restrict__ activeList,
@@ -206,8 +292,7 @@ namespace crb200
         __shared__ unsigned sCnt[64];
         __shared__ unsigned sStart[65];
         __shared__ unsigned sWarpTot;
-        __shared__ float sRec[kRec * kChunk];
-        __shared__ unsigned sMask[kChunk];
+        __shared__ unsigned sOv[65];
         __shared__ float sTile[2][4 * kTileNodes];
 
         const GridGeom &g = p.g;
@@ -240,8 +325,9 @@ namespace crb200
                     const unsigned id = (unsigned)e;
                     float rec[kRec];
                     const unsigned msk = slicers ? cutMasks[id] : 0u;
-                    if (stageParticle<Mode>(p, id, xm, vel, matParams, matType, F, Cm, V0, stride, msk, true, gridA,
-                                            gridF, fp64Count, rec))
+                    RawParticle raw;
+                    loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
+                    if (buildRecord<Mode>(p, id, raw, Cm, stride, msk, true, gridA, gridF, fp64Count, rec))
                     {
                         const Stencil st = stencilOf(g, v3(xm[id]));
                         if (Mode == 2)
@@ -317,76 +403,27 @@ namespace crb200
                     acc[n][2] = 0.f;
                     acc[n][3] = 0.f;
                 }
-                for (unsigned c0 = 0; c0 < cnt; c0 += kChunk)
+                // each cell thread walks the first kCellRun particles of its cell (id order), loading
+                // one particle ahead; capping the run keeps the lanes of a warp busy together
+                const unsigned runEnd = min(ce, cs + (unsigned)kCellRun);
+                RawParticle nxt;
+                if (cs < runEnd)
+                    loadRaw<Mode>(sIds[cs], xm, vel, matParams, matType, F, Cm, V0, stride, nxt);
+                for (unsigned q = cs; q < runEnd; ++q)
                 {
-                    for (unsigned t = tid; t < (unsigned)kChunk && c0 + t < cnt; t += 64)
-                    {
-                        const unsigned id = sIds[c0 + t];
-                        const unsigned msk = slicers ? cutMasks[id] : 0u;
-                        float rec[kRec];
-                        // outliers are scattered once, in the first pass, with global atomics
-                        const bool ok = stageParticle<Mode>(p, id, xm, vel, matParams, matType, F, Cm, V0, stride, msk,
-                                                            pass == 0, gridA, gridF, fp64Count, rec);
-                        if (!ok)
-                        {
-#pragma unroll
-                            for (int e = 0; e < kRec; ++e)
-                                rec[e] = 0.f;
-                        }
-#pragma unroll
-                        for (int e = 0; e < kRec; ++e)
-                            sRec[e * kChunk + t] = rec[e];
-                        sMask[t] = msk;
-                    }
-                    __syncthreads();
-                    const unsigned lo = max(cs, c0), hi = min(ce, c0 + (unsigned)kChunk);
-                    for (unsigned q = lo; q < hi; ++q)
-                    {
-                        const unsigned r = q - c0;
-                        const V3 u = v3(sRec[0 * kChunk + r], sRec[1 * kChunk + r], sRec[2 * kChunk + r]);
-                        const float m = sRec[3 * kChunk + r];
-                        const V3 a0 = v3(sRec[4 * kChunk + r], sRec[5 * kChunk + r], sRec[6 * kChunk + r]);
-                        const V3 a1 = v3(sRec[7 * kChunk + r], sRec[8 * kChunk + r], sRec[9 * kChunk + r]);
-                        const V3 a2 = v3(sRec[10 * kChunk + r], sRec[11 * kChunk + r], sRec[12 * kChunk + r]);
-                        const V3 fx = v3(sRec[13 * kChunk + r], sRec[14 * kChunk + r], sRec[15 * kChunk + r]);
-                        const unsigned msk = slicers ? sMask[r] : 0u;
-                        float w[3][3], dw[3][3];
-                        weights(fx, w);
-                        if (Mode == 2 && pass == 1)
-                            weightGrads(fx, dw);
-#pragma unroll
-                        for (int i = 0; i < 3; ++i)
-#pragma unroll
-                            for (int j = 0; j < 3; ++j)
-#pragma unroll
-                                for (int k = 0; k < 3; ++k)
-                                {
-                                    const int n = i * 9 + j * 3 + k;
-                                    if (slicers && ((msk >> n) & 1u))
-                                        continue;
-                                    const float wt = w[i][0] * w[j][1] * w[k][2];
-                                    if (Mode == 2 && pass == 1)
-                                    {
-                                        const float wm = wt * m;
-                                        const float gx = dw[i][0] * w[j][1] * w[k][2], gy = w[i][0] * dw[j][1] * w[k][2],
-                                                    gz = w[i][0] * w[j][1] * dw[k][2];
-                                        acc[n][0] += p.gravity.x * wm + a0.x * gx + a1.x * gy + a2.x * gz;
-                                        acc[n][1] += p.gravity.y * wm + a0.y * gx + a1.y * gy + a2.y * gz;
-                                        acc[n][2] += p.gravity.z * wm + a0.z * gx + a1.z * gy + a2.z * gz;
-                                    }
-                                    else
-                                    {
-                                        V3 val = u;
-                                        if (Mode <= 1)
-                                            val = u + a0 * (float)i + a1 * (float)j + a2 * (float)k;
-                                        acc[n][0] += val.x * wt;
-                                        acc[n][1] += val.y * wt;
-                                        acc[n][2] += val.z * wt;
-                                        acc[n][3] += m * wt;
-                                    }
-                                }
-                    }
-                    __syncthreads();
+                    const RawParticle cur = nxt;
+                    const unsigned id = sIds[q];
+                    if (q + 1 < runEnd)
+                        loadRaw<Mode>(sIds[q + 1], xm, vel, matParams, matType, F, Cm, V0, stride, nxt);
+                    const unsigned msk = slicers ? cutMasks[id] : 0u;
+                    float rec[kRec];
+                    // outliers are scattered once, in the first pass, with global atomics
+                    if (!buildRecord<Mode>(p, id, cur, Cm, stride, msk, pass == 0, gridA, gridF, fp64Count, rec))
+                        continue;
+                    if (msk)
+                        accumulateCell<Mode, true>(p, rec, msk, pass, acc);
+                    else
+                        accumulateCell<Mode, false>(p, rec, 0u, pass, acc);
                 }
                 // 4. phased flush of the registers into this warp's tile
                 float *tile = sTile[warp];
@@ -431,6 +468,53 @@ namespace crb200
                     }
                     else if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f)
                         atomicAdd(&gridA[a], make_float4(px, py, pz, m));
+                }
+                // particles beyond the first kCellRun of a cell: one per thread, vector atomics
+                {
+                    const unsigned ov = ce - runEnd;
+                    unsigned inc = ov;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1)
+                    {
+                        const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                        if (lane >= o)
+                            inc += y;
+                    }
+                    if (tid == 31)
+                        sWarpTot = inc;
+                    __syncthreads();
+                    sOv[tid + 1] = inc + (warp ? sWarpTot : 0u);
+                    if (tid == 0)
+                        sOv[0] = 0;
+                    __syncthreads();
+                    const unsigned total = sOv[64];
+                    for (unsigned kk = tid; kk < total; kk += 64)
+                    {
+                        int lo = 0, hi = 63;
+                        while (lo < hi)
+                        {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (sOv[mid] <= kk)
+                                lo = mid;
+                            else
+                                hi = mid - 1;
+                        }
+                        const unsigned id = sIds[sStart[lo] + (unsigned)kCellRun + (kk - sOv[lo])];
+                        const unsigned msk = slicers ? cutMasks[id] : 0u;
+                        RawParticle raw;
+                        loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
+                        float rec[kRec];
+                        if (buildRecord<Mode>(p, id, raw, Cm, stride, msk, pass == 0, gridA, gridF, fp64Count, rec))
+                        {
+                            const Stencil st = stencilOf(g, v3(raw.x4));
+                            if (Mode == 2 && pass == 0)
+                                scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
+                            else if (Mode == 2)
+                                scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
+                            else
+                                scatterGlobal<Mode>(p, st, rec, msk, gridA, gridF);
+                        }
+                    }
                 }
                 __syncthreads();
             }
