@@ -148,40 +148,9 @@ namespace crb200
         __syncthreads();
         for (int s = threadIdx.x; s < num; s += blockDim.x)
         {
-            const int id = shapeIds[s];
-            const int gid = sh.geometryIdx[id];
-            ShapeRec r;
-            r.pos = reinterpret_cast<const float4 *>(sh.position)[id];
-            r.rot = reinterpret_cast<const float4 *>(sh.rotation)[id];
-            r.invScale = reinterpret_cast<const float4 *>(sh.invScale)[id];
-            r.linVel = reinterpret_cast<const float4 *>(sh.linearVelocity)[id];
-            r.angVel = reinterpret_cast<const float4 *>(sh.angularVelocity)[id];
-            r.params0 = reinterpret_cast<const float4 *>(sh.params0)[id];
-            r.gparams = reinterpret_cast<const float4 *>(ge.params0)[gid];
-            r.comInvMass = sh.comInvMass ? reinterpret_cast<const float4 *>(sh.comInvMass)[id] : make_float4(0, 0, 0, 0);
-            r.inertia0 = sh.inertiaInv0 ? reinterpret_cast<const float4 *>(sh.inertiaInv0)[id] : make_float4(0, 0, 0, 0);
-            r.inertia1 = sh.inertiaInv1 ? reinterpret_cast<const float4 *>(sh.inertiaInv1)[id] : make_float4(0, 0, 0, 0);
-            r.kind = sh.type[id];
-            r.gtype = ge.type[gid];
-            r.id = id;
-            r.pad = 0;
-            {
-                // culling thresholds (sdfLowerBound), with a small safety margin
-                const float maxIsc = fmaxf(fabsf(r.invScale.x), fmaxf(fabsf(r.invScale.y), fabsf(r.invScale.z)));
-                const bool analytic = r.gtype == G_BOX || r.gtype == G_SPHERE || r.gtype == G_PLANE || r.gtype == G_CAPSULE;
-                const float band = r.params0.x + r.params0.w, pband = r.params0.w;
-                r.cull.x = (analytic && band >= 0.f && isfinite(band * maxIsc)) ? band * maxIsc * 1.0001f + 1e-6f : kMaxF32;
-                r.cull.y = (analytic && pband >= 0.f && isfinite(pband * maxIsc)) ? pband * maxIsc * 1.0001f + 1e-6f : kMaxF32;
-                r.cull.z = 0.f;
-                r.cull.w = 0.f;
-            }
+            const ShapeRec r = makeShapeRec(shapeIds[s], sh, ge);
             out[s] = r;
-            int f = 0;
-            if (r.gtype == G_QUAD_SLICER || r.gtype == G_TRIMESH_SLICER)
-                f |= SF_SLICER;
-            if (r.kind == S_DYNAMIC)
-                f |= SF_DYNAMIC;
-            atomicOr(&flags, f);
+            atomicOr(&flags, shapeFlagsOf(r));
         }
         __syncthreads();
         if (threadIdx.x == 0)
