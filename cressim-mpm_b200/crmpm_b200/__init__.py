@@ -52,6 +52,17 @@ class GeometrySdfDataC(C.Structure):
     _fields_ = [("dimension", C.c_void_p), ("lowerBoundCellSize", C.c_void_p), ("gradientSignedDistance", C.c_void_p)]
 
 
+class NoAllocStepC(C.Structure):
+    """CrB200NoAllocStep (include/crmpm_b200.h)."""
+
+    _fields_ = [("gridMin", C.c_float * 3), ("gridMax", C.c_float * 3), ("cellSize", C.c_float), ("dt", C.c_float),
+                ("gravity", C.c_float * 3), ("contactModel", C.c_int), ("numParticles", C.c_uint),
+                ("positionMass", C.c_void_p), ("velocity", C.c_void_p), ("F", C.c_void_p), ("C", C.c_void_p),
+                ("V0", C.c_void_p), ("matParams", C.c_void_p), ("matType", C.c_void_p), ("activeMask", C.c_void_p),
+                ("numShapes", C.c_int), ("shapeIds", C.c_void_p), ("shapes", ShapeDataC),
+                ("geometries", GeometryDataC), ("sdf", GeometrySdfDataC)]
+
+
 _lib = None
 
 
@@ -109,6 +120,7 @@ def lib() -> C.CDLL:
         "CrB200SolverAdvance": (i, [vp, f, vp, vp, C.POINTER(i)]),
         "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
         "CrB200SolverGetGridStats": (i, [vp, vp]),
+        "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

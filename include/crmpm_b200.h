@@ -269,6 +269,49 @@ CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[
  * and nodes that received mass (the touched-node count of the roofline byte model). */
 CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4]);
 
+/* ------------------------------------------------------------------------------------------ */
+/* MLS-MPM substep without allocation (no counterpart in the reference)                        */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Everything one allocation-free MLS-MPM substep reads and writes.  All pointers are device
+ * pointers owned by the caller.  F and C are float[9 * numParticles], column-major per particle
+ * (the layout of CrB200SolverCopyParticleState); they, positionMass and velocity are updated in
+ * place.  Grid bounds, cell size, dt, gravity, shapes and contact model mean what they mean for a
+ * solver created with CrB200SolverCreate. */
+typedef struct CrB200NoAllocStep {
+    float gridMin[3];
+    float gridMax[3];
+    float cellSize;
+    float dt;
+    float gravity[3];
+    int contactModel;
+    unsigned int numParticles;
+    CrB200Float4 *positionMass;
+    CrB200Float4 *velocity;
+    float *F;
+    float *C;
+    const float *V0;
+    const CrB200Float4 *matParams;
+    const int *matType;
+    const unsigned char *activeMask;
+    int numShapes;
+    const int *shapeIds;
+    CrB200ShapeData shapes;
+    CrB200GeometryData geometries;
+    CrB200GeometrySdfData sdf;
+} CrB200NoAllocStep;
+
+/* One MLS-MPM substep that allocates no device or host memory, for callers that cannot call
+ * cudaMalloc where they step the simulation (a host that pre-partitions all device memory, a
+ * real-time loop that must not block on an allocation, code that only owns the buffers it was
+ * handed).  This entry point has no counterpart in the reference.  Its grid scratch is a fixed
+ * static device array of 2 x 262,144 nodes (8 MiB), held by every GPU that loads the library:
+ * grids above 262,144 nodes (or more than 64 shapes) are rejected with CRB200_ERR_CAPACITY.  All
+ * calls share that array, so calls that overlap on the GPU race; serialise them.  The first call on
+ * a device looks up the array's address and should come before any stream capture.  The substep
+ * is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+CRB200_API int CrB200MlsSubstepNoAlloc(const CrB200NoAllocStep *step, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
