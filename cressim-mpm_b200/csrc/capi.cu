@@ -380,8 +380,21 @@ extern "C"
         SOLVER_OR_FAIL(solver);
         if (!masks)
             return bad("CrB200SolverCopyCutMasks: null pointer");
-        cudaError_t e = cudaMemcpyAsync(masks, s->cutMasks, s->numActive * sizeof(unsigned), cudaMemcpyDeviceToDevice,
-                                        s->stream);
+        if (!s->initialized)
+        {
+            crb200::setLastError("CrB200SolverCopyCutMasks: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        crb200::SortHeader h;
+        cudaError_t e = cudaMemcpyAsync(&h, s->header, sizeof(h), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess)
+            return crb200::cudaFail(e, "read shape flags");
+        if (s->numShapes == 0 || !(h.shapeFlags & crb200::SF_SLICER))
+            e = cudaMemsetAsync(masks, 0, s->numActive * sizeof(unsigned), s->stream); // nothing is cut
+        else
+            e = cudaMemcpyAsync(masks, s->cutMasks, s->numActive * sizeof(unsigned), cudaMemcpyDeviceToDevice, s->stream);
         return crb200::cudaFail(e, "copy cut masks");
     }
 

@@ -242,7 +242,7 @@ namespace crb200
         return acc;
     }
 
-    static __device__ __forceinline__ bool geometrySdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, V3 &grad, float &dist,
+    static __device__ __noinline__ bool geometrySdf(V3 lp, int gtype, const float4 &p0, const SdfPtrs &s, V3 &grad, float &dist,
                                              V3 &tangent)
     {
         bool inSpine = false;

@@ -109,11 +109,14 @@ namespace crb200
         unsigned char *blockFlags = nullptr;
         GridGeom *dScenes = nullptr;
         unsigned *cutMasks = nullptr;
+        float4 *records = nullptr;        // P2G records in sorted order, 4 float4 per particle
+        unsigned char *sortedCell = nullptr; // cell (0..63 in its block) of each sorted slot
         SortHeader *header = nullptr;
         ShapeRec *shapeTable = nullptr;
         unsigned totalBlocks = 0;
         unsigned numTiles = 0;
         int p2gCtas = 0;
+        int sortCtas = 0;
         int updCtas = 0;
 
         cudaGraphExec_t graph = nullptr;

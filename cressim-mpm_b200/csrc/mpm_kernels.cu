@@ -32,7 +32,6 @@ namespace crb200
     constexpr int kTileNodes = kTileEdge * kTileEdge * kTileEdge;
     constexpr int kScanTile = 256; // blocks per scan tile
     constexpr int kScanThreads = 256;
-    constexpr int kSortCap = 2048; // particles per block sorted in shared memory
 
     // ---------------------------------------------------------------------------------------
     // Addressing helpers
@@ -411,290 +410,10 @@ namespace crb200
         pairs[blockStart[key >> 6] + ranks[i]] = ((unsigned long long)(key & 63u) << 32) | i;
     }
 
-    // 5. Canonical order inside a block: bitonic sort of (local cell, id) in shared memory; larger
-    //    blocks fall back to a rank sort in global memory.
-    __global__ void __launch_bounds__(256) k_blockSort(const SortHeader *__restrict__ hdr,
-                                                       const unsigned *__restrict__ activeList,
-                                                       const unsigned *__restrict__ blockStart,
-                                                       const unsigned long long *__restrict__ pairs,
-                                                       unsigned *__restrict__ sortedIds, unsigned *status)
-    {
-        __shared__ unsigned long long s[kSortCap];
-        const unsigned nAct = hdr->numActiveBlocks;
-        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
-        {
-            const unsigned b = activeList[ab];
-            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            if (cnt <= (unsigned)kSortCap)
-            {
-                unsigned P = 1;
-                while (P < cnt)
-                    P <<= 1;
-                for (unsigned t = threadIdx.x; t < P; t += blockDim.x)
-                    s[t] = t < cnt ? pairs[start + t] : ~0ull;
-                __syncthreads();
-                for (unsigned k = 2; k <= P; k <<= 1)
-                {
-                    for (unsigned j = k >> 1; j > 0; j >>= 1)
-                    {
-                        for (unsigned t = threadIdx.x; t < P; t += blockDim.x)
-                        {
-                            const unsigned ixj = t ^ j;
-                            if (ixj > t)
-                            {
-                                const unsigned long long a = s[t], c = s[ixj];
-                                const bool up = (t & k) == 0;
-                                if ((a > c) == up)
-                                {
-                                    s[t] = c;
-                                    s[ixj] = a;
-                                }
-                            }
-                        }
-                        __syncthreads();
-                    }
-                }
-                for (unsigned t = threadIdx.x; t < cnt; t += blockDim.x)
-                    sortedIds[start + t] = (unsigned)s[t];
-                __syncthreads();
-            }
-            else
-            {
-                if (threadIdx.x == 0)
-                    atomicOr(status, CRB200_STATUS_BLOCK_OVERFLOW);
-                for (unsigned t = threadIdx.x; t < cnt; t += blockDim.x)
-                {
-                    const unsigned long long e = pairs[start + t];
-                    unsigned rank = 0;
-                    for (unsigned u = 0; u < cnt; ++u)
-                        rank += pairs[start + u] < e;
-                    sortedIds[start + rank] = (unsigned)e;
-                }
-            }
-        }
-    }
-
-    // ---------------------------------------------------------------------------------------
-    // Particle assignment inside a P2G CTA: lane l of warp w walks a contiguous chunk of the
-    // block's sorted list (chunk length q), so the 32 lanes of a warp sit in different cells and
-    // their shared-memory atomics rarely collide on a node.
-    struct ChunkWalk
-    {
-        unsigned q, lane, warp, nwarps;
-    };
-
-    __device__ __forceinline__ void tileAdd(float *tile, int t, float v) { atomicAdd(&tile[t], v); }
-
-    template <int NV>
-    __device__ __forceinline__ void flushTile(const GridGeom &g, int bx, int by, int bz, float *tile, float4 *gridA,
-                                              float4 *gridF)
-    {
-        for (int t = threadIdx.x; t < kTileNodes; t += blockDim.x)
-        {
-            const int tx = t % kTileEdge, ty = (t / kTileEdge) % kTileEdge, tz = t / (kTileEdge * kTileEdge);
-            const int i = 4 * bx + tx, j = 4 * by + ty, k = 4 * bz + tz;
-            const float m = tile[t], px = tile[kTileNodes + t], py = tile[2 * kTileNodes + t],
-                        pz = tile[3 * kTileNodes + t];
-            if (!inGrid(g, i, j, k))
-                continue;
-            const unsigned a = nodeAddr(g, i, j, k);
-            if (m != 0.f || px != 0.f || py != 0.f || pz != 0.f)
-                atomicAdd(&gridA[a], make_float4(px, py, pz, m));
-            if (NV == 7)
-            {
-                const float fx = tile[4 * kTileNodes + t], fy = tile[5 * kTileNodes + t], fz = tile[6 * kTileNodes + t];
-                if (fx != 0.f || fy != 0.f || fz != 0.f)
-                    atomicAdd(&gridF[a], make_float4(fx, fy, fz, 0.f));
-            }
-        }
-    }
-
 }
 #include "p2g_cells.cuh"
 namespace crb200
 {
-    // 6. P2G (per-particle tile atomics; kept for reference timing).  Mode 0 MLS (mls_mpm_algorithm.h:147-241), 1 PB (pb_mpm_algorithm.h:150-231),
-    //    2 standard (standard_mpm_algorithm.h:146-215).
-    template <int Mode>
-    __global__ void __launch_bounds__(128) k_p2g(StepParams p, const SortHeader *__restrict__ hdr,
-                                                 const unsigned *__restrict__ activeList,
-                                                 const unsigned *__restrict__ blockStart,
-                                                 const unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
-                                                 const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
-                                                 const int *__restrict__ matType, const float *__restrict__ F,
-                                                 float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
-                                                 const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
-                                                 float4 *__restrict__ gridA, float4 *__restrict__ gridF,
-                                                 unsigned *fp64Count)
-    {
-        constexpr int NV = Mode == 2 ? 7 : 4;
-        __shared__ float tile[NV * kTileNodes];
-        __shared__ ShapeRec sh[kMaxShapes];
-        const GridGeom &g = p.g;
-        const bool slicers = p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
-        if (slicers)
-            loadShapes(sh, shapeTable, p.numShapes);
-        const unsigned nAct = hdr->numActiveBlocks;
-        const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
-        {
-            const unsigned b = activeList[ab];
-            const unsigned lb = b - g.blockBase;
-            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
-            for (int t = threadIdx.x; t < NV * kTileNodes; t += blockDim.x)
-                tile[t] = 0.f;
-            __syncthreads();
-            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            const unsigned q = (cnt + 31) / 32;
-            for (unsigned sidx = warp; sidx < q; sidx += nwarps)
-            {
-                const unsigned jj = lane * q + sidx;
-                if (jj >= cnt)
-                    continue;
-                const unsigned id = sortedIds[start + jj];
-                const float4 x4 = xm[id];
-                const V3 x = v3(x4);
-                const float m = x4.w;
-                const Stencil st = stencilOf(g, x);
-                if (!st.finite)
-                    continue;
-                float w[3][3];
-                weights(st.fx, w);
-                const float4 v4 = vel[id];
-                V3 v = v3(v4);
-                M3 Fp, Cp;
-                loadM3(F, stride, id, Fp);
-                if (Mode != 2)
-                    loadM3(Cm, stride, id, Cp);
-                const float4 mp = matParams[id];
-                const int mt = matType[id];
-                // per-particle affine term A (momentum contribution = base + A * d)
-                M3 A;
-                V3 base;
-                float dw[3][3];
-                M3 stress;
-                if (Mode == 0)
-                {
-                    v = v + v3(p.gravity) * p.dt;
-                    stress = kirchhoffStress(Fp, mp.x, mp.y, mt);
-                    const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[id];
-#pragma unroll
-                    for (int e = 0; e < 9; ++e)
-                        A.m[e] = stress.m[e] * coef + Cp.m[e] * m;
-                    base = v * m;
-                }
-                else if (Mode == 1)
-                {
-                    if (mt == 1 || mt == 0)
-                    {
-                        // solveMaterialConstraints (constitutive_models.h:123-156)
-                        M3 tF;
-#pragma unroll
-                        for (int e = 0; e < 9; ++e)
-                            tF.m[e] = Cp.m[e] * p.dt + ((e % 4) == 0 ? 1.f : 0.f);
-                        tF = matmul(tF, Fp);
-                        const M3 R = pbRotationTarget(tF, fp64Count);
-                        const float detF = det3(tF);
-                        const float cd = fminf(fmaxf(fabsf(detF), 0.1f), 1000.0f);
-                        const float qs = 1.0f / (copysignf(1.0f, detF) * sqrtf(cd));
-                        M3 tgt;
-#pragma unroll
-                        for (int e = 0; e < 9; ++e)
-                            tgt.m[e] = R.m[e] * mp.y + (tF.m[e] * qs) * (1.0f - mp.y);
-                        const M3 TF = matmul(tgt, inverse3(Fp));
-#pragma unroll
-                        for (int e = 0; e < 9; ++e)
-                            Cp.m[e] = Cp.m[e] + ((TF.m[e] - ((e % 4) == 0 ? 1.f : 0.f)) - Cp.m[e] * p.dt) * mp.x;
-                        storeM3(Cm, stride, id, Cp);
-                    }
-                    A = Cp;
-                    base = v;
-                }
-                else
-                {
-                    weightGrads(st.fx, dw);
-                    stress = kirchhoffStress(Fp, mp.x, mp.y, mt);
-                }
-                const float v0 = Mode == 2 ? V0[id] : 0.f;
-                const int tb[3] = {st.b[0] - 4 * bx, st.b[1] - 4 * by, st.b[2] - 4 * bz};
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
-#pragma unroll
-                        for (int k = 0; k < 3; ++k)
-                        {
-                            const int ni = st.b[0] + i, nj = st.b[1] + j, nk = st.b[2] + k;
-                            if (!inGrid(g, ni, nj, nk))
-                                continue;
-                            const V3 d = v3(ex::mul(ex::sub((float)i, st.fx.x), g.dx),
-                                            ex::mul(ex::sub((float)j, st.fx.y), g.dx),
-                                            ex::mul(ex::sub((float)k, st.fx.z), g.dx));
-                            if (Mode != 2 && slicers && differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, nullptr))
-                                continue;
-                            const float wt = w[i][0] * w[j][1] * w[k][2];
-                            float vals[7];
-                            if (Mode == 2)
-                            {
-                                const float wm = wt * m;
-                                const V3 gw = v3(dw[i][0] * w[j][1] * w[k][2], w[i][0] * dw[j][1] * w[k][2],
-                                                 w[i][0] * w[j][1] * dw[k][2]);
-                                vals[0] = wm;
-                                vals[1] = v.x * wm;
-                                vals[2] = v.y * wm;
-                                vals[3] = v.z * wm;
-                                const V3 sg = v3(stress.m[0] * gw.x + stress.m[3] * gw.y + stress.m[6] * gw.z,
-                                                 stress.m[1] * gw.x + stress.m[4] * gw.y + stress.m[7] * gw.z,
-                                                 stress.m[2] * gw.x + stress.m[5] * gw.y + stress.m[8] * gw.z);
-                                vals[4] = p.gravity.x * wm + sg.x * (-v0);
-                                vals[5] = p.gravity.y * wm + sg.y * (-v0);
-                                vals[6] = p.gravity.z * wm + sg.z * (-v0);
-                            }
-                            else
-                            {
-                                const V3 ad = v3(A.m[0] * d.x + A.m[3] * d.y + A.m[6] * d.z,
-                                                 A.m[1] * d.x + A.m[4] * d.y + A.m[7] * d.z,
-                                                 A.m[2] * d.x + A.m[5] * d.y + A.m[8] * d.z);
-                                if (Mode == 0)
-                                {
-                                    vals[0] = wt * m;
-                                    vals[1] = (base.x + ad.x) * wt;
-                                    vals[2] = (base.y + ad.y) * wt;
-                                    vals[3] = (base.z + ad.z) * wt;
-                                }
-                                else
-                                {
-                                    // (v + C d) * (w m)  (pb_mpm_algorithm.h:222)
-                                    const float wm = wt * m;
-                                    vals[0] = wm;
-                                    vals[1] = (base.x + ad.x) * wm;
-                                    vals[2] = (base.y + ad.y) * wm;
-                                    vals[3] = (base.z + ad.z) * wm;
-                                }
-                            }
-                            const int tx = tb[0] + i, ty = tb[1] + j, tz = tb[2] + k;
-                            if (tx >= 0 && tx < kTileEdge && ty >= 0 && ty < kTileEdge && tz >= 0 && tz < kTileEdge)
-                            {
-                                const int t = tx + kTileEdge * (ty + kTileEdge * tz);
-#pragma unroll
-                                for (int c = 0; c < NV; ++c)
-                                    tileAdd(tile, c * kTileNodes + t, vals[c]);
-                            }
-                            else
-                            {
-                                const unsigned a = nodeAddr(g, ni, nj, nk);
-                                atomicAdd(&gridA[a], make_float4(vals[1], vals[2], vals[3], vals[0]));
-                                if (Mode == 2)
-                                    atomicAdd(&gridF[a], make_float4(vals[4], vals[5], vals[6], 0.f));
-                            }
-                        }
-            }
-            __syncthreads();
-            flushTile<NV>(g, bx, by, bz, tile, gridA, gridF);
-            __syncthreads();
-        }
-    }
-
     // 7. Grid update over touched blocks (mls_mpm_algorithm.h:243-294 and its PB / standard twins).
     __global__ void __launch_bounds__(256) k_gridUpdate(StepParams p, const SortHeader *__restrict__ hdr,
                                                         const unsigned *__restrict__ touchedList,
@@ -770,8 +489,95 @@ namespace crb200
     //    Node addresses are separable in the block-major layout (addr = AX[i] + AY[j] + AZ[k]); a
     //    particle whose stencil lies inside the grid skips all per-node bounds tests.  The APIC
     //    matrix 4/dx sum_n d_r (w v)_c is accumulated as 4/dx dx (sum_n ijk_r (w v)_c - fx_r sum_n (w v)_c).
+    // One node of the G2P gather: v += w v_n and the APIC moments (Modes 0/1) or grad v (Mode 2).
     template <int Mode>
-    __global__ void __launch_bounds__(128) k_g2p(StepParams p, const SortHeader *__restrict__ hdr,
+    __device__ __forceinline__ void g2pNode(int a, int b, int c, V3 nv, const float w[3][3], const float dw[3][3], V3 &S,
+                                            float T[9])
+    {
+        const float wt = w[a][0] * w[b][1] * w[c][2];
+        if (Mode == 2)
+        {
+            S = S + nv * wt;
+            const float gw[3] = {dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]};
+            // gradientVelocity += gw.outerProduct(nv): M(r, c) = gw_c * nv_r
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+            {
+                T[cc * 3 + 0] += gw[cc] * nv.x;
+                T[cc * 3 + 1] += gw[cc] * nv.y;
+                T[cc * 3 + 2] += gw[cc] * nv.z;
+            }
+        }
+        else
+        {
+            const V3 wv = nv * wt;
+            S = S + wv;
+            if (a)
+            {
+                T[0] += (float)a * wv.x;
+                T[1] += (float)a * wv.y;
+                T[2] += (float)a * wv.z;
+            }
+            if (b)
+            {
+                T[3] += (float)b * wv.x;
+                T[4] += (float)b * wv.y;
+                T[5] += (float)b * wv.z;
+            }
+            if (c)
+            {
+                T[6] += (float)c * wv.x;
+                T[7] += (float)c * wv.y;
+                T[8] += (float)c * wv.z;
+            }
+        }
+    }
+
+    // G2P gather for a stencil that crosses the grid boundary or has cut nodes (out of line: rare).
+    // Everything is passed and returned by value so that the caller's weights stay in registers.
+    struct G2PWeights
+    {
+        float w[3][3], dw[3][3];
+    };
+    struct G2PMoments
+    {
+        V3 S;
+        float T[9];
+    };
+
+    template <int Mode>
+    __device__ __noinline__ G2PMoments g2pGatherGeneral(GridGeom g, Stencil st, V3 x, V3 vk, unsigned msk, G2PWeights W,
+                                                        const ShapeRec *sh, int numShapes, SdfPtrs sdf,
+                                                        const float4 *__restrict__ gridV)
+    {
+        G2PMoments r;
+        r.S = v3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            r.T[e] = 0.f;
+#pragma unroll 1
+        for (int n = 0; n < 27; ++n)
+        {
+            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
+            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+            if (!inGrid(g, ni, nj, nk))
+                continue;
+            V3 nv = v3(__ldg(&gridV[nodeAddr(g, ni, nj, nk)]));
+            if (Mode != 2 && ((msk >> n) & 1u))
+            {
+                const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
+                                ex::mul(ex::sub((float)c, st.fx.z), g.dx));
+                V3 nrm;
+                if (differentSides(x, ex::add(x, d), sh, numShapes, sdf, &nrm))
+                    nv = vk - nrm * dot(vk, nrm) * 2.0f;
+            }
+            g2pNode<Mode>(a, b, c, nv, W.w, W.dw, r.S, r.T);
+        }
+        return r;
+    }
+
+    template <int Mode>
+    __global__ void __launch_bounds__(128, 6) k_g2p(StepParams p, const SortHeader *__restrict__ hdr,
                                                  float4 *__restrict__ xm, float4 *__restrict__ vel,
                                                  const unsigned char *__restrict__ mask, float *__restrict__ F,
                                                  float *__restrict__ Cm, unsigned stride,
@@ -810,59 +616,11 @@ namespace crb200
 #pragma unroll
         for (int e = 0; e < 9; ++e)
             T[e] = 0.f;
-        auto body = [&](int a, int b, int c, float4 gv) {
-            V3 nv = v3(gv);
-            if (Mode != 2 && ((msk >> (a * 9 + b * 3 + c)) & 1u))
-            {
-                const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
-                                ex::mul(ex::sub((float)c, st.fx.z), g.dx));
-                V3 nrm;
-                if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, &nrm))
-                    nv = vk - nrm * dot(vk, nrm) * 2.0f;
-            }
-            const float wt = w[a][0] * w[b][1] * w[c][2];
-            if (Mode == 2)
-            {
-                S = S + nv * wt;
-                const float gw[3] = {dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]};
-                // gradientVelocity += gw.outerProduct(nv): M(r, c) = gw_c * nv_r
-#pragma unroll
-                for (int cc = 0; cc < 3; ++cc)
-                {
-                    T[cc * 3 + 0] += gw[cc] * nv.x;
-                    T[cc * 3 + 1] += gw[cc] * nv.y;
-                    T[cc * 3 + 2] += gw[cc] * nv.z;
-                }
-            }
-            else
-            {
-                const V3 wv = nv * wt;
-                S = S + wv;
-                if (a)
-                {
-                    T[0] += (float)a * wv.x;
-                    T[1] += (float)a * wv.y;
-                    T[2] += (float)a * wv.z;
-                }
-                if (b)
-                {
-                    T[3] += (float)b * wv.x;
-                    T[4] += (float)b * wv.y;
-                    T[5] += (float)b * wv.z;
-                }
-                if (c)
-                {
-                    T[6] += (float)c * wv.x;
-                    T[7] += (float)c * wv.y;
-                    T[8] += (float)c * wv.z;
-                }
-            }
-        };
         if (st.finite)
         {
             const bool interior = st.b[0] >= 0 && st.b[0] <= g.n.x - 3 && st.b[1] >= 0 && st.b[1] <= g.n.y - 3 &&
                                   st.b[2] >= 0 && st.b[2] <= g.n.z - 3;
-            if (interior)
+            if (interior && msk == 0u)
             {
                 unsigned AX[3], AY[3], AZ[3];
 #pragma unroll
@@ -879,21 +637,24 @@ namespace crb200
                     for (int b = 0; b < 3; ++b)
 #pragma unroll
                         for (int c = 0; c < 3; ++c)
-                            body(a, b, c, __ldg(&gridV[AX[a] + AY[b] + AZ[c]]));
+                            g2pNode<Mode>(a, b, c, v3(__ldg(&gridV[AX[a] + AY[b] + AZ[c]])), w, dw, S, T);
             }
             else
             {
+                G2PWeights W;
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
+                for (int q = 0; q < 3; ++q)
 #pragma unroll
-                    for (int b = 0; b < 3; ++b)
+                    for (int d = 0; d < 3; ++d)
+                    {
+                        W.w[q][d] = w[q][d];
+                        W.dw[q][d] = Mode == 2 ? dw[q][d] : 0.f;
+                    }
+                const G2PMoments r = g2pGatherGeneral<Mode>(g, st, x, vk, msk, W, sh, p.numShapes, sdf, gridV);
+                S = r.S;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                        {
-                            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
-                            if (inGrid(g, ni, nj, nk))
-                                body(a, b, c, __ldg(&gridV[nodeAddr(g, ni, nj, nk)]));
-                        }
+                for (int e = 0; e < 9; ++e)
+                    T[e] = r.T[e];
             }
         }
         M3 Cn;
@@ -1065,18 +826,13 @@ namespace crb200
     {
         __shared__ ShapeRec sh[kMaxShapes];
         const GridGeom &g = p.g;
-        if (p.numShapes > 0)
-            loadShapes(sh, shapeTable, p.numShapes);
+        if (!(p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER)))
+            return; // no slicer in the scene: masks are neither read nor kept
+        loadShapes(sh, shapeTable, p.numShapes);
         __syncthreads();
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= p.numActive)
             return;
-        if (!(p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER)))
-        {
-            if (i < p.numActive)
-                out[i] = 0u; // no slicer in the scene: nothing is cut
-            return;
-        }
         unsigned msk = 0;
         const V3 x = v3(xm[i]);
         const Stencil st = stencilOf(g, x);
@@ -1164,7 +920,7 @@ namespace crb200
             if (e)
                 cudaEventDestroy(e);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, sortPairs, blockCount, blockStart,
-                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, dScenes};
+                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, dScenes, records, sortedCell};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -1215,6 +971,8 @@ namespace crb200
         CRB_CHECK(cudaMalloc(&header, sizeof(SortHeader)));
         CRB_CHECK(cudaMalloc(&shapeTable, kMaxShapes * sizeof(ShapeRec)));
         CRB_CHECK(cudaMalloc(&cutMasks, n * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&records, n * 4 * sizeof(float4)));
+        CRB_CHECK(cudaMalloc(&sortedCell, n));
         CRB_CHECK(cudaMemsetAsync(F, 0, 9 * n * sizeof(float), stream));
         CRB_CHECK(cudaMemsetAsync(Cm, 0, 9 * n * sizeof(float), stream));
         CRB_CHECK(cudaMemsetAsync(V0, 0, n * sizeof(float), stream));
@@ -1228,8 +986,10 @@ namespace crb200
         int dev = 0, sms = 0, perSm = 0;
         CRB_CHECK(cudaGetDevice(&dev));
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_p2gCells<0>, 64, 0));
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0>, 64, 0));
         p2gCtas = sms * (perSm > 0 ? perSm : 1);
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellSort, 64, 0));
+        sortCtas = sms * (perSm > 0 ? perSm : 1);
         updCtas = sms * 8;
         initialized = true;
         configVersion++;
@@ -1309,12 +1069,21 @@ namespace crb200
             CRB_LAUNCHED(1);
         }
         markPhase(1);
+        if (numActive > 0)
+        {
+            k_cellSort<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds, sortedCell,
+                                                    &header->status);
+            CRB_LAUNCHED(1);
+        }
         auto p2g = [&](auto mode) -> int {
             constexpr int M = decltype(mode)::value;
-            k_p2gCells<M><<<p2gCtas, 64, 0, stream>>>(p, header, activeList, blockStart, sortPairs, sortedIds, positionMass,
-                                                       velocity, matParams, matType, F, Cm, V0, stride, cutMasks, gridA,
-                                                       gridF, &header->fp64Fallbacks, &header->status);
-            CRB_LAUNCHED(1);
+            if (!pg)
+                return CRB200_OK;
+            k_record<M><<<pg, 128, 0, stream>>>(p, header, sortedIds, positionMass, velocity, matParams, matType, F, Cm, V0,
+                                                 stride, cutMasks, records, gridA, gridF, &header->fp64Fallbacks);
+            k_accumulate<M><<<p2gCtas, 64, 0, stream>>>(p, header, activeList, blockStart, sortedIds, sortedCell, records,
+                                                         cutMasks, gridA, gridF);
+            CRB_LAUNCHED(2);
             return CRB200_OK;
         };
         auto update = [&]() -> int {

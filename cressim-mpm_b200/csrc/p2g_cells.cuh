@@ -273,17 +273,15 @@ namespace crb200
         }
     }
 
-    template <int Mode>
-    __global__ void __launch_bounds__(64) k_p2gCells(StepParams p, const SortHeader *__restrict__ hdr,
-                                                     const unsigned *__restrict__ activeList,
+    // (a) Canonical order inside each active block: counting sort of the block's (cell, id) pairs
+    //     by cell, then insertion sort by id inside each cell.  Writes sortedIds and, per sorted
+    //     slot, the cell (0..63) the slot belongs to.  Blocks above kCellCap particles are ordered
+    //     by rank counting in global memory.
+    __global__ void __launch_bounds__(64) k_cellSort(const SortHeader *__restrict__ hdr, const unsigned *__restrict__ activeList,
                                                      const unsigned *__restrict__ blockStart,
                                                      const unsigned long long *__restrict__ pairs,
-                                                     unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
-                                                     const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
-                                                     const int *__restrict__ matType, const float *__restrict__ F,
-                                                     float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
-                                                     const unsigned *__restrict__ cutMasks, float4 *__restrict__ gridA,
-                                                     float4 *__restrict__ gridF, unsigned *fp64Count, unsigned *status)
+                                                     unsigned *__restrict__ sortedIds, unsigned char *__restrict__ sortedCell,
+                                                     unsigned *status)
     {
         __shared__ unsigned sIds[kCellCap];
         __shared__ unsigned sTmp[kCellCap];
@@ -292,27 +290,14 @@ namespace crb200
         __shared__ unsigned sCnt[64];
         __shared__ unsigned sStart[65];
         __shared__ unsigned sWarpTot;
-        __shared__ unsigned sOv[65];
-        __shared__ float sTile[2][4 * kTileNodes];
-
-        const GridGeom &g = p.g;
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
-        const int passes = Mode == 2 ? 2 : 1;
-        for (int t = tid; t < 2 * 4 * kTileNodes; t += 64)
-            (&sTile[0][0])[t] = 0.f;
-        __syncthreads();
         const unsigned nAct = hdr->numActiveBlocks;
-        const int cx = tid & 3, cy = (tid >> 2) & 3, cz = tid >> 4;
         for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
         {
             const unsigned b = activeList[ab];
-            const unsigned lb = b - g.blockBase;
-            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
             const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
             if (cnt > (unsigned)kCellCap)
             {
-                // oversized block: canonical order by rank counting, then per-particle global atomics
                 if (tid == 0)
                     atomicOr(status, CRB200_STATUS_BLOCK_OVERFLOW);
                 for (unsigned t = tid; t < cnt; t += 64)
@@ -322,26 +307,10 @@ namespace crb200
                     for (unsigned u2 = 0; u2 < cnt; ++u2)
                         rank += pairs[start + u2] < e;
                     sortedIds[start + rank] = (unsigned)e;
-                    const unsigned id = (unsigned)e;
-                    float rec[kRec];
-                    const unsigned msk = slicers ? cutMasks[id] : 0u;
-                    RawParticle raw;
-                    loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
-                    if (buildRecord<Mode>(p, id, raw, Cm, stride, msk, true, gridA, gridF, fp64Count, rec))
-                    {
-                        const Stencil st = stencilOf(g, v3(xm[id]));
-                        if (Mode == 2)
-                        {
-                            scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
-                            scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
-                        }
-                        else
-                            scatterGlobal<Mode>(p, st, rec, msk, gridA, gridF);
-                    }
+                    sortedCell[start + rank] = (unsigned char)(e >> 32);
                 }
                 continue;
             }
-            // 1. counting sort by cell, then by id inside each cell
             sCnt[tid] = 0;
             __syncthreads();
             for (unsigned t = tid; t < cnt; t += 64)
@@ -387,13 +356,136 @@ namespace crb200
                 }
                 sIds[j] = key;
             }
+            for (unsigned a = cs; a < ce; ++a)
+                sortedCell[start + a] = (unsigned char)tid;
             __syncthreads();
             for (unsigned t = tid; t < cnt; t += 64)
                 sortedIds[start + t] = sIds[t];
+            __syncthreads();
+        }
+    }
 
+    // (b) One record per sorted slot, particle-parallel (full occupancy).  Outliers are scattered
+    //     here with global atomics and leave a zero record.  PB-MPM's material constraint writes
+    //     the relaxed C back.
+    template <int Mode>
+    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : 8) k_record(StepParams p, const SortHeader *__restrict__ hdr,
+                                                    const unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
+                                                    const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
+                                                    const int *__restrict__ matType, const float *__restrict__ F,
+                                                    float *__restrict__ Cm, const float *__restrict__ V0, unsigned stride,
+                                                    const unsigned *__restrict__ cutMasks, float4 *__restrict__ records,
+                                                    float4 *__restrict__ gridA, float4 *__restrict__ gridF, unsigned *fp64Count)
+    {
+        const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+        if (j >= hdr->numSorted)
+            return;
+        const unsigned id = sortedIds[j];
+        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const unsigned msk = slicers ? cutMasks[id] : 0u;
+        RawParticle raw;
+        loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
+        float rec[kRec];
+        if (!buildRecord<Mode>(p, id, raw, Cm, stride, msk, true, gridA, gridF, fp64Count, rec))
+        {
+#pragma unroll
+            for (int e = 0; e < kRec; ++e)
+                rec[e] = 0.f;
+        }
+        float4 *out = records + 4ull * j;
+        out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+        out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+        out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
+        out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+    }
+
+    __device__ __forceinline__ void loadRecord(const float4 *__restrict__ records, unsigned j, float rec[kRec])
+    {
+        const float4 *r = records + 4ull * j;
+        const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+        rec[0] = a.x; rec[1] = a.y; rec[2] = a.z; rec[3] = a.w;
+        rec[4] = b.x; rec[5] = b.y; rec[6] = b.z; rec[7] = b.w;
+        rec[8] = c.x; rec[9] = c.y; rec[10] = c.z; rec[11] = c.w;
+        rec[12] = d.x; rec[13] = d.y; rec[14] = d.z; rec[15] = d.w;
+    }
+
+    // (c) Cell accumulation: one 64-thread CTA per active block, one thread per cell.
+    template <int Mode>
+    __global__ void __launch_bounds__(64) k_accumulate(StepParams p, const SortHeader *__restrict__ hdr,
+                                                       const unsigned *__restrict__ activeList,
+                                                       const unsigned *__restrict__ blockStart,
+                                                       const unsigned *__restrict__ sortedIds,
+                                                       const unsigned char *__restrict__ sortedCell,
+                                                       const float4 *__restrict__ records,
+                                                       const unsigned *__restrict__ cutMasks, float4 *__restrict__ gridA,
+                                                       float4 *__restrict__ gridF)
+    {
+        __shared__ unsigned sCnt[64];
+        __shared__ unsigned sStart[65];
+        __shared__ unsigned sOv[65];
+        __shared__ unsigned sWarpTot;
+        __shared__ float sTile[2][4 * kTileNodes];
+
+        const GridGeom &g = p.g;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const int passes = Mode == 2 ? 2 : 1;
+        for (int t = tid; t < 2 * 4 * kTileNodes; t += 64)
+            (&sTile[0][0])[t] = 0.f;
+        const unsigned nAct = hdr->numActiveBlocks;
+        const int cx = tid & 3, cy = (tid >> 2) & 3, cz = tid >> 4;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
+            // cell ranges of this block's sorted slots
+            sCnt[tid] = 0;
+            __syncthreads();
+            for (unsigned t = tid; t < cnt; t += 64)
+                atomicAdd(&sCnt[sortedCell[start + t]], 1u);
+            __syncthreads();
+            {
+                const unsigned v = sCnt[tid];
+                unsigned inc = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o)
+                        inc += y;
+                }
+                if (tid == 31)
+                    sWarpTot = inc;
+                __syncthreads();
+                const unsigned excl = inc - v + (warp ? sWarpTot : 0u);
+                sStart[tid] = excl;
+                if (tid == 63)
+                    sStart[64] = excl + v;
+                // overflow prefix: particles beyond the first kCellRun of each cell
+                const unsigned ov = v > (unsigned)kCellRun ? v - (unsigned)kCellRun : 0u;
+                unsigned oinc = ov;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, oinc, o);
+                    if (lane >= o)
+                        oinc += y;
+                }
+                __syncthreads();
+                if (tid == 31)
+                    sWarpTot = oinc;
+                __syncthreads();
+                sOv[tid + 1] = oinc + (warp ? sWarpTot : 0u);
+                if (tid == 0)
+                    sOv[0] = 0;
+            }
+            __syncthreads();
+            const unsigned cs = sStart[tid], ce = sStart[tid + 1];
+            const unsigned runEnd = min(ce, cs + (unsigned)kCellRun);
             for (int pass = 0; pass < passes; ++pass)
             {
-                // 2./3. stage and accumulate
                 float acc[27][4];
 #pragma unroll
                 for (int n = 0; n < 27; ++n)
@@ -403,29 +495,24 @@ namespace crb200
                     acc[n][2] = 0.f;
                     acc[n][3] = 0.f;
                 }
-                // each cell thread walks the first kCellRun particles of its cell (id order), loading
-                // one particle ahead; capping the run keeps the lanes of a warp busy together
-                const unsigned runEnd = min(ce, cs + (unsigned)kCellRun);
-                RawParticle nxt;
+                float nxt[kRec];
                 if (cs < runEnd)
-                    loadRaw<Mode>(sIds[cs], xm, vel, matParams, matType, F, Cm, V0, stride, nxt);
+                    loadRecord(records, start + cs, nxt);
                 for (unsigned q = cs; q < runEnd; ++q)
                 {
-                    const RawParticle cur = nxt;
-                    const unsigned id = sIds[q];
-                    if (q + 1 < runEnd)
-                        loadRaw<Mode>(sIds[q + 1], xm, vel, matParams, matType, F, Cm, V0, stride, nxt);
-                    const unsigned msk = slicers ? cutMasks[id] : 0u;
                     float rec[kRec];
-                    // outliers are scattered once, in the first pass, with global atomics
-                    if (!buildRecord<Mode>(p, id, cur, Cm, stride, msk, pass == 0, gridA, gridF, fp64Count, rec))
-                        continue;
+#pragma unroll
+                    for (int e = 0; e < kRec; ++e)
+                        rec[e] = nxt[e];
+                    if (q + 1 < runEnd)
+                        loadRecord(records, start + q + 1, nxt);
+                    const unsigned msk = slicers ? cutMasks[sortedIds[start + q]] : 0u;
                     if (msk)
                         accumulateCell<Mode, true>(p, rec, msk, pass, acc);
                     else
                         accumulateCell<Mode, false>(p, rec, 0u, pass, acc);
                 }
-                // 4. phased flush of the registers into this warp's tile
+                // phased flush of the registers into this warp's tile
                 float *tile = sTile[warp];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
@@ -443,7 +530,7 @@ namespace crb200
                             __syncwarp();
                         }
                 __syncthreads();
-                // 5. fixed-order sum of the warp tiles, one vector atomic per touched node
+                // fixed-order sum of the warp tiles, one vector atomic per touched node
                 for (int t = tid; t < kTileNodes; t += 64)
                 {
                     const float m = sTile[0][t] + sTile[1][t];
@@ -470,51 +557,36 @@ namespace crb200
                         atomicAdd(&gridA[a], make_float4(px, py, pz, m));
                 }
                 // particles beyond the first kCellRun of a cell: one per thread, vector atomics
+                const unsigned total = sOv[64];
+                for (unsigned kk = tid; kk < total; kk += 64)
                 {
-                    const unsigned ov = ce - runEnd;
-                    unsigned inc = ov;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1)
+                    int lo = 0, hi = 63;
+                    while (lo < hi)
                     {
-                        const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-                        if (lane >= o)
-                            inc += y;
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (sOv[mid] <= kk)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
                     }
-                    if (tid == 31)
-                        sWarpTot = inc;
-                    __syncthreads();
-                    sOv[tid + 1] = inc + (warp ? sWarpTot : 0u);
-                    if (tid == 0)
-                        sOv[0] = 0;
-                    __syncthreads();
-                    const unsigned total = sOv[64];
-                    for (unsigned kk = tid; kk < total; kk += 64)
-                    {
-                        int lo = 0, hi = 63;
-                        while (lo < hi)
-                        {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (sOv[mid] <= kk)
-                                lo = mid;
-                            else
-                                hi = mid - 1;
-                        }
-                        const unsigned id = sIds[sStart[lo] + (unsigned)kCellRun + (kk - sOv[lo])];
-                        const unsigned msk = slicers ? cutMasks[id] : 0u;
-                        RawParticle raw;
-                        loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
-                        float rec[kRec];
-                        if (buildRecord<Mode>(p, id, raw, Cm, stride, msk, pass == 0, gridA, gridF, fp64Count, rec))
-                        {
-                            const Stencil st = stencilOf(g, v3(raw.x4));
-                            if (Mode == 2 && pass == 0)
-                                scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
-                            else if (Mode == 2)
-                                scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
-                            else
-                                scatterGlobal<Mode>(p, st, rec, msk, gridA, gridF);
-                        }
-                    }
+                    const unsigned slot = start + sStart[lo] + (unsigned)kCellRun + (kk - sOv[lo]);
+                    float rec[kRec];
+                    loadRecord(records, slot, rec);
+                    if (rec[3] == 0.f && rec[0] == 0.f && rec[1] == 0.f && rec[2] == 0.f)
+                        continue; // zero record (outlier already scattered, or massless)
+                    Stencil st;
+                    st.b[0] = 4 * bx + (lo & 3);
+                    st.b[1] = 4 * by + ((lo >> 2) & 3);
+                    st.b[2] = 4 * bz + (lo >> 4);
+                    st.fx = v3(rec[13], rec[14], rec[15]);
+                    st.finite = true;
+                    const unsigned msk = slicers ? cutMasks[sortedIds[slot]] : 0u;
+                    if (Mode == 2 && pass == 0)
+                        scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
+                    else if (Mode == 2)
+                        scatterGlobal<3>(p, st, rec, 0u, gridA, gridF);
+                    else
+                        scatterGlobal<Mode>(p, st, rec, msk, gridA, gridF);
                 }
                 __syncthreads();
             }
