@@ -63,6 +63,14 @@ class NoAllocStepC(C.Structure):
                 ("geometries", GeometryDataC), ("sdf", GeometrySdfDataC)]
 
 
+class BatchSceneDescC(C.Structure):
+    """CrB200BatchSceneDesc (include/crmpm_b200.h)."""
+
+    _fields_ = [("gridMin", C.c_float * 3), ("gridMax", C.c_float * 3), ("cellSize", C.c_float), ("dt", C.c_float),
+                ("gravity", C.c_float * 3), ("contactModel", C.c_int), ("particleOffset", C.c_uint),
+                ("numParticles", C.c_uint), ("shapeOffset", C.c_int), ("numShapes", C.c_int)]
+
+
 _lib = None
 
 
@@ -121,6 +129,7 @@ def lib() -> C.CDLL:
         "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
         "CrB200SolverGetGridStats": (i, [vp, vp]),
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
+        "CrB200BatchCreate": (i, [i, i, vp, i, i, vp, C.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -161,6 +170,19 @@ class GpuSolver:
                                    C.c_void_p(stream or 0), C.byref(h)), "CrB200SolverCreate")
         self._h = h
         self._keep = []
+
+    @classmethod
+    def batch(cls, solver_type: int, descs, num_max_particles: int, iterations: int,
+              stream: int | None = None) -> "GpuSolver":
+        """A solver over many scenes (CrB200BatchCreate); ``descs`` is a list of BatchSceneDescC."""
+        arr = (BatchSceneDescC * len(descs))(*descs)
+        h = C.c_void_p()
+        check(lib().CrB200BatchCreate(int(solver_type), len(descs), arr, int(num_max_particles), int(iterations),
+                                      C.c_void_p(stream or 0), C.byref(h)), "CrB200BatchCreate")
+        self = cls.__new__(cls)
+        self._h = h
+        self._keep = [arr]
+        return self
 
     def release(self) -> None:
         if self._h:
@@ -326,17 +348,11 @@ class DeviceScene:
                 v = np.zeros((1,) + v.shape[1:], v.dtype)
             self.sh[k] = up(v)
         torch.cuda.synchronize(dev)
-        self.solver = GpuSolver(scene.solver_type, nm, scene.cell_size, scene.grid_min, scene.grid_max,
-                                stream=self.stream.cuda_stream)
+        self.solver = self._create_solver(scene, nm)
         s = self.solver
-        s.set_gravity(scene.gravity)
-        s.set_integration_step_size(scene.dt)
-        s.set_solver_iterations(scene.iterations)
-        s.set_shape_contact_model(scene.contact_model)
         s.bind_particle_data(self.pos.data_ptr(), self.vel.data_ptr())
         s.bind_particle_materials(self.matp.data_ptr(), self.matt.data_ptr())
         s.bind_active_mask(self.mask.data_ptr())
-        s.set_num_active_particles(n)
         p = {k: v.data_ptr() for k, v in self.sh.items()}
         s.bind_shape_data(ShapeDataC(p["shape_type"], p["geom_idx"], p["position"], p["rotation"], p["inv_scale"],
                                      p["lin_vel"], p["ang_vel"], p["com_inv_mass"], p["inertia0"], p["inertia1"],
@@ -344,10 +360,23 @@ class DeviceScene:
         s.bind_geometry_data(GeometryDataC(p["geom_type"], p["geom_params"], int(st.geom_type.shape[0])))
         s.bind_geometry_sdf_data(GeometrySdfDataC(p["sdf_dims"], p["sdf_lbcs"], p["sdf_data"]))
         s.bind_shape_ids(p["shape_ids"])
-        s.set_num_shapes(st.num_shapes)
+        self._set_counts(s, scene)
         s.initialize()
         if compute_initial:
             self.compute_initial_data()
+
+    def _create_solver(self, scene, nm: int) -> GpuSolver:
+        s = GpuSolver(scene.solver_type, nm, scene.cell_size, scene.grid_min, scene.grid_max,
+                      stream=self.stream.cuda_stream)
+        s.set_gravity(scene.gravity)
+        s.set_integration_step_size(scene.dt)
+        s.set_solver_iterations(scene.iterations)
+        s.set_shape_contact_model(scene.contact_model)
+        return s
+
+    def _set_counts(self, s: GpuSolver, scene) -> None:
+        s.set_num_active_particles(scene.n)
+        s.set_num_shapes(scene.shapes.num_shapes)
 
     def compute_initial_data(self, idx=None):
         torch = self.torch
@@ -415,3 +444,44 @@ class DeviceScene:
     def coupling(self):
         self.sync()
         return self.sh["force"].cpu().numpy(), self.sh["torque"].cpu().numpy()
+
+
+class DeviceBatch(DeviceScene):
+    """Many independent scenes advanced by one batch solver (CrB200BatchCreate).
+
+    Particles of all scenes share one set of device arrays (scene s at ``batch.slice(s)``) and
+    their shapes one merged shape table; ``state()`` returns the concatenated arrays and
+    ``scene_state(s)`` one scene's part.
+    """
+
+    def __init__(self, scene_list, device: str = "cuda:0", stream=None, compute_initial: bool = True):
+        from . import scenes as _scenes
+
+        self.batch = _scenes.make_batch(scene_list)
+        super().__init__(self.batch.merged, device=device, stream=stream, compute_initial=compute_initial)
+
+    def _create_solver(self, scene, nm: int) -> GpuSolver:
+        b = self.batch
+        descs = []
+        for k, sc in enumerate(b.scenes):
+            d = BatchSceneDescC()
+            d.gridMin[:] = [float(v) for v in sc.grid_min]
+            d.gridMax[:] = [float(v) for v in sc.grid_max]
+            d.cellSize = float(sc.cell_size)
+            d.dt = float(sc.dt)
+            d.gravity[:] = [float(v) for v in sc.gravity]
+            d.contactModel = int(sc.contact_model)
+            d.particleOffset = int(b.particle_offset[k])
+            d.numParticles = int(sc.n)
+            d.shapeOffset = int(b.shape_offset[k])
+            d.numShapes = int(sc.shapes.num_shapes)
+            descs.append(d)
+        return GpuSolver.batch(scene.solver_type, descs, nm, scene.iterations, stream=self.stream.cuda_stream)
+
+    def _set_counts(self, s: GpuSolver, scene) -> None:
+        pass  # the descriptors carry every scene's particle and shape ranges
+
+    def scene_state(self, s: int, state: dict | None = None) -> dict:
+        st = self.state() if state is None else state
+        sl = self.batch.slice(s)
+        return {k: v[sl] for k, v in st.items()}

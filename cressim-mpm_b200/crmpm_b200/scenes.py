@@ -446,3 +446,91 @@ def contact_scene(kind: str, seed: int = 1010, solver: int = SOLVER_MLS, dt: flo
         raise ValueError(kind)
     return Scene(solver, np.array([-0.3, -0.2, -0.3], np.float32), np.array([0.3, 0.4, 0.3], np.float32), cell, dt,
                  np.array([0, -9.81, 0], np.float32), 10, contact_model, pm, vel, mp, mt, mask, st, f"contact_{kind}")
+
+
+# Geometry types whose params (x, y) are (offset into the SDF data, SDF id) as int bits.
+_SDF_GEOMS = (GEOM_TRIANGLE_MESH, GEOM_TRIANGLE_MESH_SLICER, GEOM_CONNECTED_LINE_SEGMENTS)
+
+
+def _has_sdf(st: ShapeTable) -> bool:
+    return not (st.sdf_data.shape[0] == 1 and not st.sdf_data.any() and not st.sdf_dims.any())
+
+
+def merge_shape_tables(tables: list[ShapeTable]) -> tuple[ShapeTable, list[int]]:
+    """Concatenate shape tables into one (the layout a batch binds).
+
+    Shapes, geometries and SDF blocks are appended table by table; geometry indices and the SDF
+    offsets / ids inside SDF-backed geometry params are shifted accordingly.  Returns the merged
+    table and, per input table, the offset of its shape ids in the merged shape-id list.
+    """
+    out = ShapeTable.empty()
+    keys4 = ("position", "rotation", "inv_scale", "lin_vel", "ang_vel", "com_inv_mass", "inertia0", "inertia1",
+             "force", "torque", "params0")
+    sdf_dims, sdf_lbcs, sdf_data = [], [], []
+    n_sdf = n_data = 0
+    shape_offsets = []
+    ids = []
+    for st in tables:
+        s0, g0 = out.shape_type.shape[0], out.geom_type.shape[0]
+        gp = st.geom_params.copy()
+        if _has_sdf(st):
+            for gi, gt in enumerate(st.geom_type):
+                if int(gt) in _SDF_GEOMS:
+                    off, sid = gp[gi, :2].view(np.int32)
+                    gp[gi, 0] = int_bits(int(off) + n_data)
+                    gp[gi, 1] = int_bits(int(sid) + n_sdf)
+            sdf_dims.append(st.sdf_dims)
+            sdf_lbcs.append(st.sdf_lbcs)
+            sdf_data.append(st.sdf_data)
+            n_sdf += st.sdf_dims.shape[0]
+            n_data += st.sdf_data.shape[0]
+        out.geom_type = np.concatenate([out.geom_type, st.geom_type]).astype(np.int32)
+        out.geom_params = np.vstack([out.geom_params, gp]).astype(np.float32)
+        out.shape_type = np.concatenate([out.shape_type, st.shape_type]).astype(np.int32)
+        out.geom_idx = np.concatenate([out.geom_idx, st.geom_idx + g0]).astype(np.int32)
+        for k in keys4:
+            setattr(out, k, np.vstack([getattr(out, k), getattr(st, k)]).astype(np.float32))
+        shape_offsets.append(sum(len(i) for i in ids))
+        ids.append(st.shape_ids + s0)
+    out.shape_ids = np.concatenate(ids).astype(np.int32) if ids else np.zeros(0, np.int32)
+    if sdf_dims:
+        out.sdf_dims = np.vstack(sdf_dims).astype(np.int32)
+        out.sdf_lbcs = np.vstack(sdf_lbcs).astype(np.float32)
+        out.sdf_data = np.vstack(sdf_data).astype(np.float32)
+    return out, shape_offsets
+
+
+@dataclasses.dataclass
+class Batch:
+    """Scenes laid out for one batch solver: concatenated particles and shapes plus, per scene,
+    the descriptor fields of CrB200BatchSceneDesc."""
+
+    scenes: list
+    merged: Scene  # concatenated particle arrays and the merged shape table
+    particle_offset: np.ndarray  # uint32 [S]
+    shape_offset: np.ndarray  # int32 [S]
+
+    @property
+    def num_scenes(self) -> int:
+        return len(self.scenes)
+
+    def slice(self, s: int) -> slice:
+        o = int(self.particle_offset[s])
+        return slice(o, o + self.scenes[s].n)
+
+
+def make_batch(scene_list: list[Scene]) -> Batch:
+    """Lay out scenes of one solver type back to back (particles in scene order)."""
+    if not scene_list:
+        raise ValueError("a batch needs at least one scene")
+    t = scene_list[0].solver_type
+    it = scene_list[0].iterations
+    if any(s.solver_type != t or s.iterations != it for s in scene_list):
+        raise ValueError("the scenes of a batch share the solver type and iteration count")
+    offs = np.cumsum([0] + [s.n for s in scene_list[:-1]]).astype(np.uint32)
+    shapes, soffs = merge_shape_tables([s.shapes for s in scene_list])
+    cat = lambda k: np.concatenate([getattr(s, k) for s in scene_list])  # noqa: E731
+    s0 = scene_list[0]
+    merged = Scene(t, s0.grid_min, s0.grid_max, s0.cell_size, s0.dt, s0.gravity, it, s0.contact_model,
+                   cat("pos_mass"), cat("vel"), cat("mat_params"), cat("mat_type"), cat("mask"), shapes, "batch")
+    return Batch(list(scene_list), merged, offs, np.asarray(soffs, np.int32))

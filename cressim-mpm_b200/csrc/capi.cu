@@ -3,9 +3,12 @@
 // the Solver object.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <new>
 #include <thread>
+#include <utility>
+#include <vector>
 
 #include "mpm_engine.cuh"
 
@@ -76,6 +79,72 @@ extern "C"
         return CRB200_OK;
     }
 
+    CRB200_API int CrB200BatchCreate(int solverType, int numScenes, const CrB200BatchSceneDesc *scenes,
+                                     int numMaxParticles, int iterations, void *stream, CrB200SolverHandle *outSolver)
+    {
+        if (!outSolver || !scenes)
+            return bad("CrB200BatchCreate: null argument");
+        *outSolver = nullptr;
+        if (solverType != CRB200_SOLVER_GPU_MLS && solverType != CRB200_SOLVER_GPU_PB &&
+            solverType != CRB200_SOLVER_GPU_STANDARD)
+        {
+            crb200::setLastError("CrB200BatchCreate: only the GPU solver types (1, 3, 5) are provided");
+            return CRB200_ERR_UNSUPPORTED;
+        }
+        if (numScenes <= 0 || numScenes > 65535)
+            return bad("CrB200BatchCreate: numScenes must be in [1, 65535]");
+        if (numMaxParticles <= 0 || iterations < 0)
+            return bad("CrB200BatchCreate: numMaxParticles must be positive and iterations non-negative");
+        // particle ranges: inside the arrays and pairwise disjoint
+        std::vector<std::pair<unsigned, unsigned>> ranges;
+        double nodes = 0.0;
+        for (int i = 0; i < numScenes; ++i)
+        {
+            const CrB200BatchSceneDesc &d = scenes[i];
+            if (!(d.cellSize > 0.f) || !(d.dt > 0.f))
+                return bad("CrB200BatchCreate: cellSize and dt must be positive");
+            for (int a = 0; a < 3; ++a)
+                if (!(d.gridMax[a] > d.gridMin[a]))
+                    return bad("CrB200BatchCreate: empty grid bounds");
+            if (d.contactModel != CRB200_CONTACT_KINEMATIC && d.contactModel != CRB200_CONTACT_EFFECTIVE_MASS)
+                return bad("CrB200BatchCreate: unknown contact model");
+            if ((unsigned long long)d.particleOffset + d.numParticles > (unsigned long long)numMaxParticles)
+            {
+                crb200::setLastError("CrB200BatchCreate: a particle range exceeds numMaxParticles");
+                return CRB200_ERR_CAPACITY;
+            }
+            if (d.numShapes < 0 || d.shapeOffset < 0)
+                return bad("CrB200BatchCreate: negative shape range");
+            if (d.numShapes > crb200::kMaxShapes)
+            {
+                crb200::setLastError("CrB200BatchCreate: at most 64 shapes per scene");
+                return CRB200_ERR_CAPACITY;
+            }
+            if (d.numParticles)
+                ranges.emplace_back(d.particleOffset, d.particleOffset + d.numParticles);
+            const crb200::GridGeom g = crb200::makeGridGeom(d.cellSize, d.gridMin, d.gridMax, 0);
+            if (g.n.x < 5 || g.n.y < 5 || g.n.z < 5)
+                return bad("CrB200BatchCreate: every grid needs at least 5 nodes per dimension");
+            nodes += 64.0 * g.nb.x * g.nb.y * (double)g.nb.z;
+        }
+        std::sort(ranges.begin(), ranges.end());
+        for (size_t i = 1; i < ranges.size(); ++i)
+            if (ranges[i].first < ranges[i - 1].second)
+                return bad("CrB200BatchCreate: particle ranges of two scenes overlap");
+        if (nodes >= 4294967295.0)
+        {
+            crb200::setLastError("CrB200BatchCreate: the scenes' grids exceed 2^32 nodes together");
+            return CRB200_ERR_CAPACITY;
+        }
+        Solver *s = new (std::nothrow)
+            Solver(solverType, numMaxParticles, scenes, numScenes, iterations, static_cast<cudaStream_t>(stream));
+        if (!s)
+            return bad("CrB200BatchCreate: out of host memory");
+        CrB200Solver *h = new (std::nothrow) CrB200Solver{s};
+        *outSolver = h;
+        return CRB200_OK;
+    }
+
     CRB200_API int CrB200SolverRelease(CrB200SolverHandle solver)
     {
         SOLVER_OR_FAIL(solver);
@@ -124,8 +193,14 @@ extern "C"
     {
         SOLVER_OR_FAIL(solver);
         s->gravity = make_float3(gx, gy, gz);
+        for (auto &d : s->batch)
+        {
+            d.gravity[0] = gx;
+            d.gravity[1] = gy;
+            d.gravity[2] = gz;
+        }
         s->configVersion++;
-        return CRB200_OK;
+        return s->uploadParams();
     }
 
     CRB200_API int CrB200SolverSetIntegrationStepSize(CrB200SolverHandle solver, float dt)
@@ -134,8 +209,10 @@ extern "C"
         if (!(dt > 0.f))
             return bad("CrB200SolverSetIntegrationStepSize: dt must be positive");
         s->dt = dt;
+        for (auto &d : s->batch)
+            d.dt = dt;
         s->configVersion++;
-        return CRB200_OK;
+        return s->uploadParams();
     }
 
     CRB200_API int CrB200SolverSetSolverIterations(CrB200SolverHandle solver, int iterations)
@@ -154,13 +231,20 @@ extern "C"
         if (contactModel != CRB200_CONTACT_KINEMATIC && contactModel != CRB200_CONTACT_EFFECTIVE_MASS)
             return bad("CrB200SolverSetShapeContactModel: unknown contact model");
         s->contactModel = contactModel;
+        for (auto &d : s->batch)
+            d.contactModel = contactModel;
         s->configVersion++;
-        return CRB200_OK;
+        return s->uploadParams();
     }
 
     CRB200_API int CrB200SolverSetNumActiveParticles(CrB200SolverHandle solver, unsigned int n)
     {
         SOLVER_OR_FAIL(solver);
+        if (s->isBatch())
+        {
+            crb200::setLastError("CrB200SolverSetNumActiveParticles: a batch takes its particle ranges from its scenes");
+            return CRB200_ERR_UNSUPPORTED;
+        }
         if (n > (unsigned)s->numMaxParticles)
         {
             crb200::setLastError("CrB200SolverSetNumActiveParticles: more than numMaxParticles");
@@ -209,6 +293,11 @@ extern "C"
     CRB200_API int CrB200SolverSetNumShapes(CrB200SolverHandle solver, int numShapes)
     {
         SOLVER_OR_FAIL(solver);
+        if (s->isBatch())
+        {
+            crb200::setLastError("CrB200SolverSetNumShapes: a batch takes its shape ranges from its scenes");
+            return CRB200_ERR_UNSUPPORTED;
+        }
         if (numShapes < 0)
             return bad("CrB200SolverSetNumShapes: negative");
         if (numShapes > crb200::kMaxShapes)
@@ -391,10 +480,11 @@ extern "C"
             e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "read shape flags");
-        if (s->numShapes == 0 || !(h.shapeFlags & crb200::SF_SLICER))
-            e = cudaMemsetAsync(masks, 0, s->numActive * sizeof(unsigned), s->stream); // nothing is cut
+        const unsigned n = s->totalParticles();
+        if (s->numShapes == 0 || (!s->isBatch() && !(h.shapeFlags & crb200::SF_SLICER)))
+            e = cudaMemsetAsync(masks, 0, n * sizeof(unsigned), s->stream); // nothing is cut
         else
-            e = cudaMemcpyAsync(masks, s->cutMasks, s->numActive * sizeof(unsigned), cudaMemcpyDeviceToDevice, s->stream);
+            e = cudaMemcpyAsync(masks, s->cutMasks, n * sizeof(unsigned), cudaMemcpyDeviceToDevice, s->stream);
         return crb200::cudaFail(e, "copy cut masks");
     }
 

@@ -25,6 +25,10 @@ namespace crb200
         unsigned blockBase;
     };
 
+    // Everything a kernel needs to know about one scene.  A solver holds one (the reference's
+    // single-scene solvers) or many (the batch); particles of scene s occupy
+    // [particleBegin, particleBegin + numActive) of the shared particle arrays and its shapes are
+    // shapeTable[shapeBegin, shapeBegin + numShapes).
     struct StepParams
     {
         GridGeom g;
@@ -35,6 +39,20 @@ namespace crb200
         int solverType;
         unsigned numActive;
         int numShapes;
+        unsigned particleBegin;
+        int shapeBegin;
+        int pad;
+    };
+
+    // Scene lookup handed to every kernel.  With one scene the kernels use their StepParams
+    // argument and never touch these tables.
+    struct SceneTable
+    {
+        const StepParams *params;            // numScenes entries
+        const unsigned short *particleScene; // scene of each particle (0xFFFF: none)
+        unsigned *flags;                     // SF_* shape flags per scene
+        int numScenes;
+        unsigned numParticles;               // particles covered by all scenes
     };
 
     // Device-side sort / bookkeeping header (one per solver).
@@ -55,6 +73,9 @@ namespace crb200
     public:
         Solver(int solverType, int numMaxParticles, float cellSize, const float gmin[3], const float gmax[3],
                cudaStream_t stream);
+        // A batch of independent scenes sharing particle and shape arrays (CrB200BatchCreate).
+        Solver(int solverType, int numMaxParticles, const CrB200BatchSceneDesc *scenes, int numScenes, int iterations,
+               cudaStream_t stream);
         ~Solver();
 
         int initialize();
@@ -69,6 +90,16 @@ namespace crb200
         int solverType;
         int numMaxParticles;
         GridGeom geom;
+        // batch: per-scene descriptors, grids and ranges (empty for a single-scene solver)
+        std::vector<CrB200BatchSceneDesc> batch;
+        std::vector<GridGeom> batchGeom;
+        StepParams *dParams = nullptr;
+        unsigned short *dParticleScene = nullptr;
+        unsigned *dSceneFlags = nullptr;
+        bool isBatch() const { return !batch.empty(); }
+        int numScenes() const { return isBatch() ? (int)batch.size() : 1; }
+        unsigned totalParticles() const;
+        int totalShapes() const;
         cudaStream_t stream;
         float dt = 0.002f; // MpmSolverBase default (mpm_solver_base.h:146)
         float3 gravity = {0.f, 0.f, 0.f};
@@ -107,7 +138,7 @@ namespace crb200
         unsigned *activeList = nullptr, *touchedList = nullptr;
         unsigned *tileSums = nullptr;
         unsigned char *blockFlags = nullptr;
-        GridGeom *dScenes = nullptr;
+
         unsigned *cutMasks = nullptr;
         float4 *records = nullptr;        // P2G records in sorted order, 4 float4 per particle
         unsigned char *sortedCell = nullptr; // cell (0..63 in its block) of each sorted slot
@@ -124,10 +155,18 @@ namespace crb200
         int graphKernels = 0;
 
         StepParams params() const;
+        SceneTable sceneTable() const;
+        std::vector<StepParams> allParams() const;
+        int uploadParams();
         int launchStep();   // enqueue one step's kernels
+        template <bool Multi>
+        int launchStepT();
         int sortParticles(const StepParams &p, bool ignoreMask);
         void gatherShapes();
     };
+
+    // Grid of one scene (node counts as the reference's solver constructors compute them).
+    GridGeom makeGridGeom(float cellSize, const float gmin[3], const float gmax[3], unsigned blockBase);
 
     // error plumbing shared by the C ABI
     void setLastError(const std::string &msg);

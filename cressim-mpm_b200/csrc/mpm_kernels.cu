@@ -18,6 +18,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <string>
@@ -136,44 +137,69 @@ namespace crb200
             d[t] = s[t];
     }
 
+    // Scene of a block (binary search over the scenes' block bases; scene 0 for one scene).
+    __device__ __forceinline__ int sceneOfBlock(const SceneTable &sc, unsigned b)
+    {
+        int lo = 0, hi = sc.numScenes - 1;
+        while (lo < hi)
+        {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sc.params[mid].g.blockBase <= b)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+
     // ---------------------------------------------------------------------------------------
     // 1. Shape table
-    __global__ void k_gatherShapes(int num, const int *__restrict__ shapeIds, CrB200ShapeData sh, CrB200GeometryData ge,
-                                   ShapeRec *__restrict__ out, SortHeader *hdr)
+    __global__ void k_gatherShapes(const __grid_constant__ StepParams p, SceneTable sc, const int *__restrict__ shapeIds, CrB200ShapeData sh,
+                                   CrB200GeometryData ge, ShapeRec *__restrict__ out)
     {
         __shared__ int flags;
+        const int scene = blockIdx.x;
+        const StepParams &sp = sc.numScenes > 1 ? sc.params[scene] : p;
         if (threadIdx.x == 0)
             flags = 0;
         __syncthreads();
-        for (int s = threadIdx.x; s < num; s += blockDim.x)
+        for (int s = threadIdx.x; s < sp.numShapes; s += blockDim.x)
         {
-            const ShapeRec r = makeShapeRec(shapeIds[s], sh, ge);
-            out[s] = r;
+            const int t = sp.shapeBegin + s;
+            const ShapeRec r = makeShapeRec(shapeIds[t], sh, ge);
+            out[t] = r;
             atomicOr(&flags, shapeFlagsOf(r));
         }
         __syncthreads();
         if (threadIdx.x == 0)
-            hdr->shapeFlags = (unsigned)flags;
+            sc.flags[scene] = (unsigned)flags;
     }
 
     // ---------------------------------------------------------------------------------------
     // 2. Bin: cell keys and warp-aggregated block histogram (rank = arrival order in its block).
-    __global__ void k_bin(GridGeom g, unsigned numActive, bool ignoreMask, const float4 *__restrict__ xm,
+    template <bool Multi>
+    __global__ void k_bin(const __grid_constant__ StepParams p, SceneTable sc, bool ignoreMask, const float4 *__restrict__ xm,
                           const unsigned char *__restrict__ mask, unsigned *__restrict__ keys,
                           unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount, SortHeader *hdr)
     {
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         const unsigned lane = threadIdx.x & 31;
+        const unsigned n = Multi ? sc.numParticles : p.numActive;
         unsigned key = kInvalidKey;
         bool ood = false;
-        if (i < numActive && (ignoreMask || mask[i]))
+        if (i < n && (ignoreMask || mask[i]))
         {
-            const float4 x = xm[i];
-            const Stencil s = stencilOf(g, v3(x));
-            if (s.finite)
-                key = cellKey(g, s, &ood);
-            else
-                ood = true;
+            const unsigned short si = Multi ? sc.particleScene[i] : 0;
+            if (!Multi || si != 0xFFFF)
+            {
+                const GridGeom &g = Multi ? sc.params[si].g : p.g;
+                const float4 x = xm[i];
+                const Stencil s = stencilOf(g, v3(x));
+                if (s.finite)
+                    key = cellKey(g, s, &ood);
+                else
+                    ood = true;
+            }
         }
         const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
         const unsigned peers = __match_any_sync(0xffffffffu, blk);
@@ -182,7 +208,7 @@ namespace crb200
         if (blk != kInvalidKey && (int)lane == leader)
             base = atomicAdd(&blockCount[blk], (unsigned)__popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (i < numActive)
+        if (i < n)
         {
             keys[i] = key;
             ranks[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
@@ -195,21 +221,7 @@ namespace crb200
     // 3. Scan over blocks.  Tile t covers blocks [t*kScanTile, (t+1)*kScanTile).
     //    flags bit 0: block holds particles; bit 1: block holds nodes some particle touches
     //    (the block itself or one of its -x/-y/-z neighbours holds particles).
-    __device__ __forceinline__ const GridGeom &sceneOfBlock(const GridGeom *scenes, int numScenes, unsigned b)
-    {
-        int lo = 0, hi = numScenes - 1;
-        while (lo < hi)
-        {
-            const int mid = (lo + hi + 1) >> 1;
-            if (scenes[mid].blockBase <= b)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        return scenes[lo];
-    }
-
-    __global__ void k_scanReduce(const GridGeom *__restrict__ scenes, int numScenes, unsigned totalBlocks,
+    __global__ void k_scanReduce(StepParams p, SceneTable sc, unsigned totalBlocks,
                                  const unsigned *__restrict__ blockCount, unsigned char *__restrict__ flags,
                                  uint3 *__restrict__ tileSums)
     {
@@ -220,7 +232,7 @@ namespace crb200
             const unsigned b = b0 + e;
             if (b >= totalBlocks)
                 break;
-            const GridGeom &g = sceneOfBlock(scenes, numScenes, b);
+            const GridGeom &g = sc.numScenes > 1 ? sc.params[sceneOfBlock(sc, b)].g : p.g;
             const unsigned lb = b - g.blockBase;
             const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
             const unsigned c = blockCount[b];
@@ -415,20 +427,22 @@ namespace crb200
 namespace crb200
 {
     // 7. Grid update over touched blocks (mls_mpm_algorithm.h:243-294 and its PB / standard twins).
-    __global__ void __launch_bounds__(256) k_gridUpdate(StepParams p, const SortHeader *__restrict__ hdr,
+    //    Multi: the touched blocks belong to many scenes; each block reads its scene's parameters
+    //    and shapes from global memory (single scene: kernel arguments and shared memory).
+    template <bool Multi>
+    __global__ void __launch_bounds__(256) k_gridUpdate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                         const unsigned *__restrict__ touchedList,
                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                         float4 *__restrict__ gridA, float4 *__restrict__ gridF,
                                                         float4 *__restrict__ gridV, float4 *coupleForce,
                                                         float4 *coupleTorque)
     {
-        __shared__ ShapeRec sh[kMaxShapes];
-        const GridGeom &g = p.g;
-        if (p.numShapes > 0)
-            loadShapes(sh, shapeTable, p.numShapes);
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
+            loadShapes(sh, shapeTable, p0.numShapes);
         __syncthreads();
         const unsigned nT = hdr->numTouchedBlocks;
-        const bool withForce = p.solverType == CRB200_SOLVER_GPU_STANDARD;
+        const bool withForce = p0.solverType == CRB200_SOLVER_GPU_STANDARD;
         const unsigned perCta = blockDim.x / 64;
         for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
         {
@@ -436,6 +450,9 @@ namespace crb200
             if (bi >= nT)
                 continue;
             const unsigned b = touchedList[bi];
+            const StepParams &p = Multi ? sc.params[sceneOfBlock(sc, b)] : p0;
+            const GridGeom &g = p.g;
+            const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
             const unsigned l = threadIdx.x & 63;
             const unsigned lb = b - g.blockBase;
             const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
@@ -473,7 +490,7 @@ namespace crb200
             V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z);
             pos = pos + v * p.dt;
             if (p.numShapes > 0)
-                rigidContact<false>(v, acc.w, pos, sh, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque);
+                rigidContact<false>(v, acc.w, pos, shp, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque);
             if (i < 2 || i > g.n.x - 3)
                 v.x = 0.f;
             if (j < 2 || j > g.n.y - 3)
@@ -576,26 +593,30 @@ namespace crb200
         return r;
     }
 
-    template <int Mode>
-    __global__ void __launch_bounds__(128, 6) k_g2p(StepParams p, const SortHeader *__restrict__ hdr,
-                                                 float4 *__restrict__ xm, float4 *__restrict__ vel,
-                                                 const unsigned char *__restrict__ mask, float *__restrict__ F,
-                                                 float *__restrict__ Cm, unsigned stride,
+    template <int Mode, bool Multi>
+    __global__ void __launch_bounds__(128, 6) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
+                                                 float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
+                                                 float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                  const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
                                                  unsigned *status)
     {
-        __shared__ ShapeRec sh[kMaxShapes];
-        const GridGeom &g = p.g;
-        if (p.numShapes > 0)
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
         {
-            loadShapes(sh, shapeTable, p.numShapes);
+            loadShapes(sh, shapeTable, p0.numShapes);
             __syncthreads();
         }
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= p.numActive || !mask[i])
+        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
             return;
-        const bool slicers = Mode != 2 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && si == 0xFFFFu)
+            return;
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const GridGeom &g = p.g;
+        const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
+        const bool slicers = Mode != 2 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
         const float4 x4 = xm[i];
         const V3 x = v3(x4);
         const Stencil st = stencilOf(g, x);
@@ -650,7 +671,7 @@ namespace crb200
                         W.w[q][d] = w[q][d];
                         W.dw[q][d] = Mode == 2 ? dw[q][d] : 0.f;
                     }
-                const G2PMoments r = g2pGatherGeneral<Mode>(g, st, x, vk, msk, W, sh, p.numShapes, sdf, gridV);
+                const G2PMoments r = g2pGatherGeneral<Mode>(g, st, x, vk, msk, W, shp, p.numShapes, sdf, gridV);
                 S = r.S;
 #pragma unroll
                 for (int e = 0; e < 9; ++e)
@@ -688,7 +709,7 @@ namespace crb200
                 fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
         V3 vn = va;
         if (p.numShapes > 0)
-            rigidContact<true>(vn, x4.w, xn, sh, p.numShapes, sdf, false, nullptr, nullptr);
+            rigidContact<true>(vn, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr);
         M3 Fp, Mu;
         loadM3(F, stride, i, Fp);
 #pragma unroll
@@ -705,20 +726,26 @@ namespace crb200
     }
 
     // PB-MPM integration (pb_mpm_algorithm.h:363-408).
-    __global__ void __launch_bounds__(128) k_pbIntegrate(StepParams p, float4 *__restrict__ xm, float4 *__restrict__ vel,
-                                                         const unsigned char *__restrict__ mask, float *__restrict__ F,
-                                                         const float *__restrict__ Cm, unsigned stride,
-                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
-                                                         unsigned *status)
+    template <bool Multi>
+    __global__ void __launch_bounds__(128) k_pbIntegrate(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
+                                                         float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
+                                                         float *__restrict__ F, const float *__restrict__ Cm,
+                                                         unsigned stride, const ShapeRec *__restrict__ shapeTable,
+                                                         SdfPtrs sdf, unsigned *status)
     {
-        __shared__ ShapeRec sh[kMaxShapes];
-        const GridGeom &g = p.g;
-        if (p.numShapes > 0)
-            loadShapes(sh, shapeTable, p.numShapes);
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
+            loadShapes(sh, shapeTable, p0.numShapes);
         __syncthreads();
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= p.numActive || !mask[i])
+        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
             return;
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && si == 0xFFFFu)
+            return;
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const GridGeom &g = p.g;
+        const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
         const float4 x4 = xm[i];
         V3 v = v3(vel[i]);
         V3 xn = v3(x4) + v * p.dt;
@@ -726,7 +753,7 @@ namespace crb200
                 fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
         v = v + v3(p.gravity) * p.dt;
         if (p.numShapes > 0)
-            rigidContact<true>(v, x4.w, xn, sh, p.numShapes, sdf, false, nullptr, nullptr);
+            rigidContact<true>(v, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr);
         M3 Fp, Cp, Mu;
         loadM3(F, stride, i, Fp);
         loadM3(Cm, stride, i, Cp);
@@ -744,13 +771,16 @@ namespace crb200
     // ---------------------------------------------------------------------------------------
     // computeInitialData (mls_mpm_algorithm.h:46-145): F = I, mass scatter, volume gather, then the
     // accumulation grid is cleared again.
-    __global__ void k_initMass(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+    __global__ void k_initMass(GridGeom g0, SceneTable sc, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
                                float *__restrict__ F, unsigned stride, float4 *__restrict__ gridA)
     {
         const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
         if (ii >= n)
             return;
         const unsigned p = idx[ii];
+        if (sc.particleScene && sc.particleScene[p] == 0xFFFFu)
+            return;
+        const GridGeom g = sc.particleScene ? sc.params[sc.particleScene[p]].g : g0;
         M3 I;
 #pragma unroll
         for (int e = 0; e < 9; ++e)
@@ -773,13 +803,16 @@ namespace crb200
                 }
     }
 
-    __global__ void k_initVolume(GridGeom g, unsigned n, const unsigned *__restrict__ idx,
+    __global__ void k_initVolume(GridGeom g0, SceneTable sc, unsigned n, const unsigned *__restrict__ idx,
                                  const float4 *__restrict__ xm, const float4 *__restrict__ gridA, float *__restrict__ V0)
     {
         const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
         if (ii >= n)
             return;
         const unsigned p = idx[ii];
+        if (sc.particleScene && sc.particleScene[p] == 0xFFFFu)
+            return;
+        const GridGeom g = sc.particleScene ? sc.params[sc.particleScene[p]].g : g0;
         const float4 x4 = xm[p];
         const Stencil st = stencilOf(g, v3(x4));
         float dens = 0.f;
@@ -800,13 +833,17 @@ namespace crb200
         V0[p] = dens > 1e-8f ? x4.w / dens : 1e-8f;
     }
 
-    __global__ void k_initClear(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+    __global__ void k_initClear(GridGeom g0, SceneTable sc, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
                                 float4 *__restrict__ gridA)
     {
         const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
         if (ii >= n)
             return;
-        const Stencil st = stencilOf(g, v3(xm[idx[ii]]));
+        const unsigned p = idx[ii];
+        if (sc.particleScene && sc.particleScene[p] == 0xFFFFu)
+            return;
+        const GridGeom g = sc.particleScene ? sc.params[sc.particleScene[p]].g : g0;
+        const Stencil st = stencilOf(g, v3(xm[p]));
         if (!st.finite)
             return;
         for (int a = 0; a < 3; ++a)
@@ -820,19 +857,32 @@ namespace crb200
     }
 
     // Cut masks of the current positions (bit a*9 + b*3 + c), for inspection.
-    __global__ void k_cutMasks(StepParams p, const SortHeader *__restrict__ hdr, const float4 *__restrict__ xm,
+    //    Multi: every particle gets a mask (zero in scenes without a slicer).
+    template <bool Multi>
+    __global__ void k_cutMasks(const __grid_constant__ StepParams p0, SceneTable sc, const float4 *__restrict__ xm,
                                const unsigned char *__restrict__ mask, const ShapeRec *__restrict__ shapeTable,
                                SdfPtrs sdf, unsigned *__restrict__ out)
     {
-        __shared__ ShapeRec sh[kMaxShapes];
-        const GridGeom &g = p.g;
-        if (!(p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER)))
-            return; // no slicer in the scene: masks are neither read nor kept
-        loadShapes(sh, shapeTable, p.numShapes);
-        __syncthreads();
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi)
+        {
+            if (!(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER)))
+                return; // no slicer in the scene: masks are neither read nor kept
+            loadShapes(sh, shapeTable, p0.numShapes);
+            __syncthreads();
+        }
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= p.numActive)
+        if (i >= (Multi ? sc.numParticles : p0.numActive))
             return;
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && (si == 0xFFFFu || !(sc.flags[si] & SF_SLICER)))
+        {
+            out[i] = 0u;
+            return;
+        }
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const GridGeom &g = p.g;
+        const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
         unsigned msk = 0;
         const V3 x = v3(xm[i]);
         const Stencil st = stencilOf(g, x);
@@ -846,7 +896,7 @@ namespace crb200
                             continue;
                         const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
                                         ex::mul(ex::sub((float)c, st.fx.z), g.dx));
-                        if (differentSides(x, ex::add(x, d), sh, p.numShapes, sdf, nullptr))
+                        if (differentSides(x, ex::add(x, d), shp, p.numShapes, sdf, nullptr))
                             msk |= 1u << (a * 9 + b * 3 + c);
                     }
         }
@@ -888,8 +938,7 @@ namespace crb200
             return cudaFail(e_, "kernel launch");           \
     } while (0)
 
-    Solver::Solver(int type, int nmax, float cellSize, const float mn[3], const float mx[3], cudaStream_t s)
-        : solverType(type), numMaxParticles(nmax), stream(s)
+    GridGeom makeGridGeom(float cellSize, const float mn[3], const float mx[3], unsigned blockBase)
     {
         // Node counts exactly like the reference constructor (gpu_mls_mpm_solver.cu:40-52):
         // int((max - min) / dx + 1) in single precision.
@@ -900,16 +949,118 @@ namespace crb200
             volatile float q = size / cellSize;
             dims[d] = q + 1.0f;
         }
-        geom.gmin = make_float3(mn[0], mn[1], mn[2]);
-        geom.gmax = make_float3(mx[0], mx[1], mx[2]);
-        geom.dx = cellSize;
-        geom.invDx = 1 / cellSize;
-        geom.cellVol = cellSize * cellSize * cellSize;
-        geom.n = make_int3((int)dims[0], (int)dims[1], (int)dims[2]);
-        geom.nb = make_int3((geom.n.x + 5) >> 2, (geom.n.y + 5) >> 2, (geom.n.z + 5) >> 2);
-        geom.blockBase = 0;
+        GridGeom g;
+        g.gmin = make_float3(mn[0], mn[1], mn[2]);
+        g.gmax = make_float3(mx[0], mx[1], mx[2]);
+        g.dx = cellSize;
+        g.invDx = 1 / cellSize;
+        g.cellVol = cellSize * cellSize * cellSize;
+        g.n = make_int3((int)dims[0], (int)dims[1], (int)dims[2]);
+        g.nb = make_int3((g.n.x + 5) >> 2, (g.n.y + 5) >> 2, (g.n.z + 5) >> 2);
+        g.blockBase = blockBase;
+        return g;
+    }
+
+    Solver::Solver(int type, int nmax, float cellSize, const float mn[3], const float mx[3], cudaStream_t s)
+        : solverType(type), numMaxParticles(nmax), stream(s)
+    {
+        geom = makeGridGeom(cellSize, mn, mx, 0);
         totalBlocks = (unsigned)geom.nb.x * geom.nb.y * geom.nb.z;
         numTiles = (totalBlocks + kScanTile - 1) / kScanTile;
+    }
+
+    // Scenes are laid out back to back: grids in block order (scene s owns blocks
+    // [blockBase_s, blockBase_s + nb_s)), particles and shapes at the descriptor's offsets.
+    Solver::Solver(int type, int nmax, const CrB200BatchSceneDesc *scenes, int n, int iters, cudaStream_t s)
+        : solverType(type), numMaxParticles(nmax), stream(s)
+    {
+        batch.assign(scenes, scenes + n);
+        iterations = iters;
+        unsigned base = 0;
+        for (int i = 0; i < n; ++i)
+        {
+            const GridGeom g = makeGridGeom(scenes[i].cellSize, scenes[i].gridMin, scenes[i].gridMax, base);
+            batchGeom.push_back(g);
+            base += (unsigned)g.nb.x * g.nb.y * g.nb.z;
+        }
+        geom = batchGeom[0];
+        dt = scenes[0].dt;
+        gravity = make_float3(scenes[0].gravity[0], scenes[0].gravity[1], scenes[0].gravity[2]);
+        contactModel = scenes[0].contactModel;
+        numActive = totalParticles();
+        numShapes = totalShapes();
+        totalBlocks = base;
+        numTiles = (totalBlocks + kScanTile - 1) / kScanTile;
+    }
+
+    unsigned Solver::totalParticles() const
+    {
+        if (!isBatch())
+            return numActive;
+        unsigned n = 0;
+        for (const auto &d : batch)
+            n = std::max(n, (unsigned)(d.particleOffset + d.numParticles));
+        return n;
+    }
+
+    int Solver::totalShapes() const
+    {
+        if (!isBatch())
+            return numShapes;
+        int n = 0;
+        for (const auto &d : batch)
+            n = std::max(n, d.shapeOffset + d.numShapes);
+        return n;
+    }
+
+    std::vector<StepParams> Solver::allParams() const
+    {
+        std::vector<StepParams> out;
+        if (!isBatch())
+        {
+            out.push_back(params());
+            return out;
+        }
+        for (size_t i = 0; i < batch.size(); ++i)
+        {
+            const CrB200BatchSceneDesc &d = batch[i];
+            StepParams p;
+            p.g = batchGeom[i];
+            p.dt = d.dt;
+            p.gravity = make_float3(d.gravity[0], d.gravity[1], d.gravity[2]);
+            p.cutoff = solverType == CRB200_SOLVER_GPU_PB ? 1e-8f : 1e-4f;
+            p.contactModel = d.contactModel;
+            p.solverType = solverType;
+            p.numActive = (unsigned)d.numParticles;
+            p.numShapes = d.numShapes;
+            p.particleBegin = (unsigned)d.particleOffset;
+            p.shapeBegin = d.shapeOffset;
+            p.pad = 0;
+            out.push_back(p);
+        }
+        return out;
+    }
+
+    // Scene parameters live on the device for batches; setters re-upload them between substeps.
+    int Solver::uploadParams()
+    {
+        if (!isBatch() || !dParams)
+            return CRB200_OK;
+        const std::vector<StepParams> ps = allParams();
+        CRB_CHECK(cudaStreamSynchronize(stream));
+        CRB_CHECK(cudaMemcpy(dParams, ps.data(), ps.size() * sizeof(StepParams), cudaMemcpyHostToDevice));
+        return CRB200_OK;
+    }
+
+    SceneTable Solver::sceneTable() const
+    {
+        SceneTable t;
+        t.params = dParams;
+        t.particleScene = dParticleScene;
+        t.flags = isBatch() ? dSceneFlags : &header->shapeFlags;
+        t.numScenes = numScenes();
+        t.numParticles = totalParticles();
+        return t;
     }
 
     Solver::~Solver()
@@ -920,7 +1071,8 @@ namespace crb200
             if (e)
                 cudaEventDestroy(e);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, sortPairs, blockCount, blockStart,
-                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, dScenes, records, sortedCell};
+                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, sortedCell,
+                        dParams, dParticleScene, dSceneFlags};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -937,6 +1089,9 @@ namespace crb200
         p.solverType = solverType;
         p.numActive = numActive;
         p.numShapes = numShapes;
+        p.particleBegin = 0;
+        p.shapeBegin = 0;
+        p.pad = 0;
         return p;
     }
 
@@ -966,10 +1121,23 @@ namespace crb200
         CRB_CHECK(cudaMalloc(&touchedList, totalBlocks * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&tileSums, numTiles * sizeof(uint3)));
         CRB_CHECK(cudaMalloc(&blockFlags, totalBlocks));
-        CRB_CHECK(cudaMalloc(&dScenes, sizeof(GridGeom)));
-        CRB_CHECK(cudaMemcpyAsync(dScenes, &geom, sizeof(GridGeom), cudaMemcpyHostToDevice, stream));
         CRB_CHECK(cudaMalloc(&header, sizeof(SortHeader)));
-        CRB_CHECK(cudaMalloc(&shapeTable, kMaxShapes * sizeof(ShapeRec)));
+        const int shapeSlots = isBatch() ? std::max(totalShapes(), 1) : kMaxShapes;
+        CRB_CHECK(cudaMalloc(&shapeTable, shapeSlots * sizeof(ShapeRec)));
+        if (isBatch())
+        {
+            std::vector<unsigned short> owner(n, 0xFFFF);
+            for (size_t i = 0; i < batch.size(); ++i)
+                for (int q = 0; q < batch[i].numParticles; ++q)
+                    owner[batch[i].particleOffset + q] = (unsigned short)i;
+            CRB_CHECK(cudaMalloc(&dParams, batch.size() * sizeof(StepParams)));
+            CRB_CHECK(cudaMalloc(&dParticleScene, n * sizeof(unsigned short)));
+            CRB_CHECK(cudaMalloc(&dSceneFlags, batch.size() * sizeof(unsigned)));
+            CRB_CHECK(cudaMemcpy(dParticleScene, owner.data(), n * sizeof(unsigned short), cudaMemcpyHostToDevice));
+            CRB_CHECK(cudaMemset(dSceneFlags, 0, batch.size() * sizeof(unsigned)));
+            const std::vector<StepParams> ps = allParams();
+            CRB_CHECK(cudaMemcpy(dParams, ps.data(), ps.size() * sizeof(StepParams), cudaMemcpyHostToDevice));
+        }
         CRB_CHECK(cudaMalloc(&cutMasks, n * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&records, n * 4 * sizeof(float4)));
         CRB_CHECK(cudaMalloc(&sortedCell, n));
@@ -986,7 +1154,7 @@ namespace crb200
         int dev = 0, sms = 0, perSm = 0;
         CRB_CHECK(cudaGetDevice(&dev));
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0>, 64, 0));
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0, false>, 64, 0));
         p2gCtas = sms * (perSm > 0 ? perSm : 1);
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellSort, 64, 0));
         sortCtas = sms * (perSm > 0 ? perSm : 1);
@@ -998,20 +1166,26 @@ namespace crb200
 
     void Solver::gatherShapes()
     {
-        k_gatherShapes<<<1, 64, 0, stream>>>(numShapes, shapeIds, shapes, geometries, shapeTable, header);
+        k_gatherShapes<<<numScenes(), 64, 0, stream>>>(params(), sceneTable(), shapeIds, shapes, geometries, shapeTable);
     }
 
     int Solver::sortParticles(const StepParams &p, bool ignoreMask)
     {
-        const unsigned n = numActive;
+        const SceneTable sc = sceneTable();
+        const unsigned n = sc.numParticles;
         const unsigned pg = (n + 127) / 128;
         if (n > 0)
         {
-            k_bin<<<pg, 128, 0, stream>>>(p.g, n, ignoreMask, positionMass, activeMask, keys, ranks, blockCount, header);
+            if (isBatch())
+                k_bin<true><<<pg, 128, 0, stream>>>(p, sc, ignoreMask, positionMass, activeMask, keys, ranks, blockCount,
+                                                    header);
+            else
+                k_bin<false><<<pg, 128, 0, stream>>>(p, sc, ignoreMask, positionMass, activeMask, keys, ranks, blockCount,
+                                                     header);
             CRB_LAUNCHED(1);
         }
         unsigned char *flags = blockFlags;
-        k_scanReduce<<<numTiles, kScanThreads, 0, stream>>>(dScenes, 1, totalBlocks, blockCount, flags,
+        k_scanReduce<<<numTiles, kScanThreads, 0, stream>>>(p, sc, totalBlocks, blockCount, flags,
                                                             reinterpret_cast<uint3 *>(tileSums));
         k_scanTiles<<<1, 1024, 0, stream>>>(reinterpret_cast<uint3 *>(tileSums), numTiles, header);
         k_scanWrite<<<numTiles, kScanThreads, 0, stream>>>(totalBlocks, reinterpret_cast<const uint3 *>(tileSums),
@@ -1030,7 +1204,15 @@ namespace crb200
 {
     int Solver::launchStep()
     {
-        if (numShapes > kMaxShapes)
+        if (isBatch())
+            return launchStepT<true>();
+        return launchStepT<false>();
+    }
+
+    template <bool Multi>
+    int Solver::launchStepT()
+    {
+        if (!Multi && numShapes > kMaxShapes)
         {
             setLastError("step: more than 64 shapes in one scene");
             return CRB200_ERR_CAPACITY;
@@ -1046,6 +1228,8 @@ namespace crb200
             return CRB200_ERR_NOT_INITIALIZED;
         }
         const StepParams p = params();
+        const SceneTable sc = sceneTable();
+        const unsigned nPart = sc.numParticles;
         markPhase(0);
         if (numShapes > 0)
         {
@@ -1056,7 +1240,7 @@ namespace crb200
                          reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
         float4 *cf = reinterpret_cast<float4 *>(shapes.force), *ct = reinterpret_cast<float4 *>(shapes.torque);
         const unsigned stride = (unsigned)numMaxParticles;
-        const unsigned pg = (numActive + 127) / 128;
+        const unsigned pg = (nPart + 127) / 128;
         const bool isStd = solverType == CRB200_SOLVER_GPU_STANDARD;
         int r = sortParticles(p, isStd);
         if (r != CRB200_OK)
@@ -1065,11 +1249,11 @@ namespace crb200
         // iterations, so one evaluation serves every iteration of the step).
         if (numShapes > 0 && !isStd && pg)
         {
-            k_cutMasks<<<pg, 128, 0, stream>>>(p, header, positionMass, activeMask, shapeTable, sp, cutMasks);
+            k_cutMasks<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, shapeTable, sp, cutMasks);
             CRB_LAUNCHED(1);
         }
         markPhase(1);
-        if (numActive > 0)
+        if (nPart > 0)
         {
             k_cellSort<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds, sortedCell,
                                                     &header->status);
@@ -1079,15 +1263,17 @@ namespace crb200
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
-            k_record<M><<<pg, 128, 0, stream>>>(p, header, sortedIds, positionMass, velocity, matParams, matType, F, Cm, V0,
-                                                 stride, cutMasks, records, gridA, gridF, &header->fp64Fallbacks);
-            k_accumulate<M><<<p2gCtas, 64, 0, stream>>>(p, header, activeList, blockStart, sortedIds, sortedCell, records,
-                                                         cutMasks, gridA, gridF);
+            k_record<M, Multi><<<pg, 128, 0, stream>>>(p, sc, header, sortedIds, positionMass, velocity, matParams, matType,
+                                                        F, Cm, V0, stride, cutMasks, records, gridA, gridF,
+                                                        &header->fp64Fallbacks);
+            k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, sortedCell,
+                                                                records, cutMasks, gridA, gridF);
             CRB_LAUNCHED(2);
             return CRB200_OK;
         };
         auto update = [&]() -> int {
-            k_gridUpdate<<<updCtas, 256, 0, stream>>>(p, header, touchedList, shapeTable, sp, gridA, gridF, gridV, cf, ct);
+            k_gridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV,
+                                                             cf, ct);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1095,8 +1281,8 @@ namespace crb200
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
-            k_g2p<M><<<pg, 128, 0, stream>>>(p, header, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
-                                             gridV, cutMasks, &header->status);
+            k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
+                                                    sp, gridV, cutMasks, &header->status);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1123,8 +1309,8 @@ namespace crb200
             }
             if (pg)
             {
-                k_pbIntegrate<<<pg, 128, 0, stream>>>(p, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp,
-                                                      &header->status);
+                k_pbIntegrate<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride,
+                                                             shapeTable, sp, &header->status);
                 CRB_LAUNCHED(1);
             }
         }
@@ -1169,6 +1355,12 @@ namespace crb200
 
     int Solver::advance(float dtFrame, float4 *hostX, float4 *hostV, int *outSubsteps)
     {
+        for (const auto &d : batch)
+            if (d.dt != dt)
+            {
+                setLastError("advance: the scenes of this batch have different substep sizes");
+                return CRB200_ERR_UNSUPPORTED;
+            }
         // scene_impl.cpp:313-317: float time accumulation decides the substep count
         float t = 0.f;
         int n = 0;
@@ -1180,10 +1372,11 @@ namespace crb200
         int r = stepMany(n);
         if (r != CRB200_OK)
             return r;
-        if (hostX && numActive)
-            CRB_CHECK(cudaMemcpyAsync(hostX, positionMass, numActive * sizeof(float4), cudaMemcpyDeviceToHost, stream));
-        if (hostV && numActive)
-            CRB_CHECK(cudaMemcpyAsync(hostV, velocity, numActive * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        const unsigned nPart = totalParticles();
+        if (hostX && nPart)
+            CRB_CHECK(cudaMemcpyAsync(hostX, positionMass, nPart * sizeof(float4), cudaMemcpyDeviceToHost, stream));
+        if (hostV && nPart)
+            CRB_CHECK(cudaMemcpyAsync(hostV, velocity, nPart * sizeof(float4), cudaMemcpyDeviceToHost, stream));
         CRB_CHECK(cudaStreamSynchronize(stream));
         if (outSubsteps)
             *outSubsteps = n;
@@ -1269,9 +1462,10 @@ namespace crb200
             return CRB200_ERR_INVALID_ARGUMENT;
         }
         const unsigned g = (n + 127) / 128;
-        k_initMass<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, F, (unsigned)numMaxParticles, gridA);
-        k_initVolume<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, gridA, V0);
-        k_initClear<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, gridA);
+        const SceneTable sc = sceneTable();
+        k_initMass<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, F, (unsigned)numMaxParticles, gridA);
+        k_initVolume<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA, V0);
+        k_initClear<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA);
         CRB_LAUNCHED(3);
         return CRB200_OK;
     }

@@ -368,8 +368,9 @@ namespace crb200
     // (b) One record per sorted slot, particle-parallel (full occupancy).  Outliers are scattered
     //     here with global atomics and leave a zero record.  PB-MPM's material constraint writes
     //     the relaxed C back.
-    template <int Mode>
-    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : 8) k_record(StepParams p, const SortHeader *__restrict__ hdr,
+    template <int Mode, bool Multi>
+    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : 8) k_record(const __grid_constant__ StepParams p0, SceneTable sc,
+                                                    const SortHeader *__restrict__ hdr,
                                                     const unsigned *__restrict__ sortedIds, const float4 *__restrict__ xm,
                                                     const float4 *__restrict__ vel, const float4 *__restrict__ matParams,
                                                     const int *__restrict__ matType, const float *__restrict__ F,
@@ -381,7 +382,9 @@ namespace crb200
         if (j >= hdr->numSorted)
             return;
         const unsigned id = sortedIds[j];
-        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
+        const unsigned si = Multi ? sc.particleScene[id] : 0u; // sorted particles have a scene
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const bool slicers = Mode <= 1 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
         const unsigned msk = slicers ? cutMasks[id] : 0u;
         RawParticle raw;
         loadRaw<Mode>(id, xm, vel, matParams, matType, F, Cm, V0, stride, raw);
@@ -410,8 +413,9 @@ namespace crb200
     }
 
     // (c) Cell accumulation: one 64-thread CTA per active block, one thread per cell.
-    template <int Mode>
-    __global__ void __launch_bounds__(64) k_accumulate(StepParams p, const SortHeader *__restrict__ hdr,
+    //     Multi: each active block reads its scene's parameters (block base search).
+    template <int Mode, bool Multi>
+    __global__ void __launch_bounds__(64) k_accumulate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                        const unsigned *__restrict__ activeList,
                                                        const unsigned *__restrict__ blockStart,
                                                        const unsigned *__restrict__ sortedIds,
@@ -426,9 +430,7 @@ namespace crb200
         __shared__ unsigned sWarpTot;
         __shared__ float sTile[2][4 * kTileNodes];
 
-        const GridGeom &g = p.g;
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        const bool slicers = Mode <= 1 && p.numShapes > 0 && (hdr->shapeFlags & SF_SLICER);
         const int passes = Mode == 2 ? 2 : 1;
         for (int t = tid; t < 2 * 4 * kTileNodes; t += 64)
             (&sTile[0][0])[t] = 0.f;
@@ -437,6 +439,10 @@ namespace crb200
         for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
         {
             const unsigned b = activeList[ab];
+            const unsigned si = Multi ? (unsigned)sceneOfBlock(sc, b) : 0u;
+            const StepParams &p = Multi ? sc.params[si] : p0;
+            const GridGeom &g = p.g;
+            const bool slicers = Mode <= 1 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
             const unsigned lb = b - g.blockBase;
             const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
             const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;

@@ -270,6 +270,39 @@ CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[
 CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4]);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Batches of independent scenes (SimulationFactory::advanceAll, simulation_factory_impl.cpp:  */
+/* 235-261 and 1106-1150, which loops over per-scene solvers; here all scenes advance in one   */
+/* launch per phase)                                                                           */
+/* ------------------------------------------------------------------------------------------ */
+
+/* One scene of a batch: its grid, integration parameters, and its ranges in the shared particle
+ * arrays and in the shared shape-id list.  Particle ranges of different scenes must not overlap. */
+typedef struct CrB200BatchSceneDesc {
+    float gridMin[3];
+    float gridMax[3];
+    float cellSize;
+    float dt;
+    float gravity[3];
+    int contactModel;
+    unsigned int particleOffset;
+    unsigned int numParticles;
+    int shapeOffset;
+    int numShapes;
+} CrB200BatchSceneDesc;
+
+/* Create a solver that advances `numScenes` independent scenes together: every phase of a step
+ * is one launch over all scenes (CrB200SolverStepMany replays it as one CUDA graph).  The returned
+ * handle takes the ordinary solver calls: bind the shared particle, material, mask, shape-id,
+ * shape, geometry and SDF arrays (ids in shape-id lists are global shape ids), Initialize,
+ * ComputeInitialData (particle indices are global), Step / StepMany, CopyParticleState, Release.
+ * All scenes share the solver type and PB-MPM iteration count; SetGravity /
+ * SetIntegrationStepSize / SetShapeContactModel apply to every scene; the particle and shape
+ * counts come from the descriptors (SetNumActiveParticles / SetNumShapes are refused). */
+CRB200_API int CrB200BatchCreate(int solverType, int numScenes, const CrB200BatchSceneDesc *scenes,
+                                 int numMaxParticles, int iterations, void *stream,
+                                 CrB200SolverHandle *outSolver);
+
+/* ------------------------------------------------------------------------------------------ */
 /* MLS-MPM substep without allocation (no counterpart in the reference)                        */
 /* ------------------------------------------------------------------------------------------ */
 
