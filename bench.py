@@ -237,13 +237,13 @@ def run_ours(args, rank, world, local):
     substep_bytes = 200.0 * n + 64.0 * touched_nodes
     substep_gbs = substep_bytes / (ms / 1e3 / args.steps) / 1e9
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     if os.path.exists(tfile):
-        try:
-            with open(tfile) as f:
-                traffic = json.load(f).get(args.workload, {}).get(dom)
-        except Exception:
-            traffic = None
+        with open(tfile) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and not line.startswith("#") and parts[:2] == [args.workload, dom]:
+                    traffic = float(parts[2])
 
     # end to end through the C ABI: scene-style advance with host buffers
     frame_substeps = 10

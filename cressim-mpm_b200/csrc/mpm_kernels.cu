@@ -1252,13 +1252,13 @@ namespace crb200
             k_cutMasks<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, shapeTable, sp, cutMasks);
             CRB_LAUNCHED(1);
         }
-        markPhase(1);
         if (nPart > 0)
         {
             k_cellSort<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds, sortedCell,
                                                     &header->status);
             CRB_LAUNCHED(1);
         }
+        markPhase(1);
         auto p2g = [&](auto mode) -> int {
             constexpr int M = decltype(mode)::value;
             if (!pg)

@@ -259,8 +259,9 @@ CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int 
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the
  * solver stream since the last reset, and the number of substeps they cover.  Phases:
- * 0 shape gather + binning + scan + sort, 1 P2G, 2 grid update, 3 G2P (PB-MPM: G2P plus the
- * integration kernel).  Synchronizes the solver stream. */
+ * 0 shape gather + binning + scan + scatter + cut masks + per-block cell sort, 1 P2G (particle
+ * records + cell accumulation), 2 grid update, 3 G2P (PB-MPM: G2P plus the integration kernel).
+ * Synchronizes the solver stream. */
 #define CRB200_NUM_PHASES 4
 CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[CRB200_NUM_PHASES],
                                          int *outSubsteps, int reset);
