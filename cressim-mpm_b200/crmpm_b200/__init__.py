@@ -130,6 +130,8 @@ def lib() -> C.CDLL:
         "CrB200SolverGetGridStats": (i, [vp, vp]),
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
         "CrB200BatchCreate": (i, [i, i, vp, i, i, vp, C.POINTER(vp)]),
+        "CrB200SolverAdjointRecord": (i, [vp, i, i, i, vp, vp]),
+        "CrB200SolverAdjointBackward": (i, [vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -302,6 +304,15 @@ class GpuSolver:
         n = C.c_int()
         check(lib().CrB200SolverGetPhaseTimes(self._h, ms, C.byref(n), int(reset)), "phase_times")
         return list(ms), n.value
+
+    def adjoint_record(self, num_substeps: int, interval: int, captures, captured_ptr: int):
+        caps = (C.c_int * max(len(captures), 1))(*[int(t) for t in captures])
+        check(lib().CrB200SolverAdjointRecord(self._h, int(num_substeps), int(interval), len(captures), caps,
+                                              C.c_void_p(captured_ptr)), "adjoint_record")
+
+    def adjoint_backward(self, grad_ptr: int, grad_v_ptr: int = 0, grad_mat_ptr: int = 0, grad_x_ptr: int = 0):
+        check(lib().CrB200SolverAdjointBackward(self._h, C.c_void_p(grad_ptr), C.c_void_p(grad_v_ptr),
+                                                C.c_void_p(grad_mat_ptr), C.c_void_p(grad_x_ptr)), "adjoint_backward")
 
     def grid_stats(self):
         out = (C.c_uint * 4)()

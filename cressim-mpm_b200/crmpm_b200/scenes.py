@@ -326,11 +326,15 @@ def batched_scenes(seed: int = 1004, num_scenes: int = 256, cells: int = 64, cel
 
 
 def material_cube(seed: int = 1005, side: float = 0.4, cell: float = 0.02, ppc: int = 8, E: float = 2e4,
-                  nu: float = 0.35, rho: float = 1000.0, dt: float = 2e-4, v0=(0.0, 0.0, 0.0)) -> Scene:
-    """64k-particle cube over a ground plane for material identification (dx 0.02, 20 cells/side)."""
+                  nu: float = 0.35, rho: float = 1000.0, dt: float = 2e-4, v0=(0.0, 0.0, 0.0),
+                  drop: float = 0.05) -> Scene:
+    """64k-particle cube over a ground plane for material identification (dx 0.02, 20 cells/side).
+
+    The cube's lower face starts ``drop`` above the plane and moves with initial velocity ``v0``.
+    """
     lam, mu = lame(E, nu)
     h = side / 2
-    pos = jittered_box((-h, 0.05, -h), (h, 0.05 + side, h), cell, ppc, seed)
+    pos = jittered_box((-h, drop, -h), (h, drop + side, h), cell, ppc, seed)
     mass = rho * cell ** 3 / ppc
     pm, vel, mp, mt, mask = _particles(pos, mass, (lam, mu, 0, 0), MAT_NEOHOOKEAN)
     vel[:, :3] = np.asarray(v0, np.float32)
@@ -534,3 +538,31 @@ def make_batch(scene_list: list[Scene]) -> Batch:
     merged = Scene(t, s0.grid_min, s0.grid_max, s0.cell_size, s0.dt, s0.gravity, it, s0.contact_model,
                    cat("pos_mass"), cat("vel"), cat("mat_params"), cat("mat_type"), cat("mask"), shapes, "batch")
     return Batch(list(scene_list), merged, offs, np.asarray(soffs, np.int32))
+
+
+def adjoint_scene(kind: str = "plane", seed: int = 1006, side: float = 0.1, cell: float = 0.02,
+                  v0=(0.3, -1.5, 0.2), E: float = 2e4, nu: float = 0.35) -> Scene:
+    """A 1000-particle Neo-Hookean cube 5 mm above the ground moving at v0, for gradient checks.
+
+    kind "plane": the ground plane only.  kind "mixed": the plane, a kinematic sphere (translating
+    and spinning), a static box and a tilted static capsule around the impact point, with smoothing
+    distances and drags that put grid nodes in every contact branch.
+    """
+    sc = material_cube(seed=seed, side=side, cell=cell, E=E, nu=nu, v0=v0, drop=0.005)
+    if kind == "mixed":
+        st = ShapeTable.empty()
+        g = st.add_geometry(GEOM_PLANE, (0, 0, 0, 0))
+        st.add_shape(g, SHAPE_STATIC, (0, 0, 0), friction=0.3)
+        g = st.add_geometry(GEOM_SPHERE, (0.04, 0, 0, 0))
+        st.add_shape(g, SHAPE_KINEMATIC, (0.03, -0.02, 0.0), smooth=0.02, drag=0.8, friction=0.3,
+                     lin_vel=(0, 0.2, 0), ang_vel=(0, 1.0, 0.5))
+        g = st.add_geometry(GEOM_BOX, (0.03, 0.02, 0.03, 0))
+        st.add_shape(g, SHAPE_STATIC, (-0.04, -0.005, 0.02), smooth=0.02, drag=0.9, friction=0.4)
+        g = st.add_geometry(GEOM_CAPSULE, (0.015, 0.03, 0, 0))
+        c, s_ = math.cos(0.6), math.sin(0.6)
+        st.add_shape(g, SHAPE_STATIC, (0.0, 0.0, -0.04), rotation=(s_, 0, 0, c), smooth=0.02, drag=0.9, friction=0.2)
+        sc.shapes = st
+    elif kind != "plane":
+        raise ValueError(kind)
+    sc.name = f"adjoint_{kind}"
+    return sc

@@ -1,0 +1,826 @@
+// Adjoint of the MLS-MPM substep (no counterpart in the reference, which has no gradient path).
+//
+// Forward map of one substep, state (x, v, F, C) per particle, parameters (lambda, mu) per particle:
+//   P2G          P_n += w_n (m (v + g dt) + A d_n),  M_n += w_n m,  A = -dt 4/dx^2 V0 tau(F) + m C
+//                (mls_mpm_algorithm.h:147-241; tau Neo-Hookean, constitutive_models.h:62-75)
+//   grid update  V_n = P_n / M_n, rigid contact at x_n + V_n dt, two-node boundary band; nodes below
+//                the 1e-4 mass cutoff keep their momentum (mls_mpm_algorithm.h:243-294)
+//   G2P          v' = sum w_n V_n, C' = 4/dx sum w_n d_n V_n^T, x' = clamp(x + v' dt) then the
+//                particle push-out, F' = (I + dt C') F (mls_mpm_algorithm.h:296-390)
+// The reverse substep runs three kernels in the opposite order, after replaying the forward P2G and
+// grid update of that substep from its recomputed input state:
+//   k_adjG2P         per particle: adjoint of G2P; scatters dL/dV_n to the adjoint grid
+//   k_adjGridUpdate  per touched node: adjoint of the division and of the contact chain -> dL/dP_n, dL/dM_n
+//   k_adjP2G         per particle: gathers dL/dP_n, dL/dM_n; adjoint of P2G and of the stress
+// Branch decisions (contact on/off, friction clamp, position clamp, mass cutoff) are those of the
+// replayed forward and are held fixed.  Scope: MLS-MPM, Neo-Hookean particles, the kinematic contact
+// model, analytic shapes (box, sphere, plane, capsule) of uniform scale, no slicers.
+#pragma once
+
+namespace crb200
+{
+    constexpr int kAdjMaxHits = 8; // contacts per particle / node that one reverse step can undo
+
+    // Signed distance, unit normal and the local frame quantities of shape r at world point pos,
+    // exactly as rigidContact evaluates them (mpm_rigid_contact.h:129-148).
+    __device__ __forceinline__ bool adjShapeEval(const ShapeRec &r, V3 pos, const SdfPtrs &sdf, float &dist, V3 &n,
+                                                 V3 &lp, V3 &gl)
+    {
+        const V3 isc = v3(r.invScale);
+        const V3 wrel = pos - v3(r.pos);
+        lp = mul(qrotInv(r.rot, wrel), isc);
+        V3 grad, tangent = v3(0.f, 0.f, 0.f);
+        float d;
+        geometrySdf(lp, r.gtype, r.gparams, sdf, grad, d, tangent);
+        if (isnan(d))
+            return false;
+        gl = grad;
+        grad = mul(grad, isc);
+        const float is = rsqrtf(sq(grad));
+        dist = d * is - r.params0.w;
+        n = qrot(r.rot, grad * is);
+        return true;
+    }
+
+    // d(normal)/d(pos) in world space, row-major J[3 i + j] = dn_i / dpos_j, for the analytic
+    // geometries of uniform scale s: J = s R J_local R^T.
+    __device__ __forceinline__ void adjNormalJacobian(const ShapeRec &r, V3 lp, V3 gl, float J[9])
+    {
+        float L[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            L[e] = 0.f;
+        const float4 p0 = r.gparams;
+        if (r.gtype == G_SPHERE || r.gtype == G_CAPSULE)
+        {
+            V3 pa = lp;
+            bool slide = false;
+            if (r.gtype == G_CAPSULE)
+            {
+                const float h2 = p0.y * 2.f;
+                pa.y -= p0.y;
+                const float h = fminf(fmaxf(-pa.y / h2, 0.f), 1.f);
+                slide = h > 0.f && h < 1.f;
+                pa.y += h2 * h;
+            }
+            const float ln = fmaxf(sqrtf(sq(pa)), kEps);
+            const float g[3] = {gl.x, gl.y, gl.z};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    L[3 * i + j] = (slide && j == 1) ? 0.f : ((i == j ? 1.f : 0.f) - g[i] * g[j]) / ln;
+        }
+        else if (r.gtype == G_BOX)
+        {
+            const float pen[3] = {fabsf(lp.x) - p0.x, fabsf(lp.y) - p0.y, fabsf(lp.z) - p0.z};
+            const float sg[3] = {lp.x < 0.f ? -1.f : 1.f, lp.y < 0.f ? -1.f : 1.f, lp.z < 0.f ? -1.f : 1.f};
+            const float gm = fmaxf(pen[0], fmaxf(pen[1], pen[2]));
+            if (gm > 0.f)
+            {
+                const float q[3] = {fmaxf(pen[0], 0.f), fmaxf(pen[1], 0.f), fmaxf(pen[2], 0.f)};
+                const float l = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+                const float dir[3] = {q[0] / l, q[1] / l, q[2] / l};
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j)
+                        L[3 * i + j] = sg[i] * (((i == j ? 1.f : 0.f) - dir[i] * dir[j]) / l) * (pen[j] > 0.f ? sg[j] : 0.f);
+            }
+        }
+        // R columns
+        const V3 c0 = qrot(r.rot, v3(1.f, 0.f, 0.f)), c1 = qrot(r.rot, v3(0.f, 1.f, 0.f)), c2 = qrot(r.rot, v3(0.f, 0.f, 1.f));
+        const float R[9] = {c0.x, c1.x, c2.x, c0.y, c1.y, c2.y, c0.z, c1.z, c2.z}; // row-major
+        float T[9];                                                              // L R^T
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                T[3 * i + j] = L[3 * i] * R[3 * j] + L[3 * i + 1] * R[3 * j + 1] + L[3 * i + 2] * R[3 * j + 2];
+        const float s = r.invScale.x;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                J[3 * i + j] = s * (R[3 * i] * T[j] + R[3 * i + 1] * T[3 + j] + R[3 * i + 2] * T[6 + j]);
+    }
+
+    // J^T g for a row-major 3x3 J
+    __device__ __forceinline__ V3 adjJtG(const float J[9], V3 g)
+    {
+        return v3(J[0] * g.x + J[3] * g.y + J[6] * g.z, J[1] * g.x + J[4] * g.y + J[7] * g.z,
+                  J[2] * g.x + J[5] * g.y + J[8] * g.z);
+    }
+
+    __device__ __forceinline__ void loadAdj9(const float *planes, unsigned stride, unsigned i, float m[9])
+    {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            m[k] = planes[k * stride + i];
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Reverse of G2P (per particle).  In: adjoint of the substep's output state in aX, aV, aF, aC.
+    // Out: aX, aF hold the G2P part of the adjoint of the input x and F; dL/dV_n is added to gridG.
+    template <bool Multi>
+    __global__ void __launch_bounds__(128) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
+                                                   const float4 *__restrict__ xm, const unsigned char *__restrict__ mask,
+                                                   const float *__restrict__ F, unsigned stride,
+                                                   const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                   const float4 *__restrict__ gridV, float4 *__restrict__ aX,
+                                                   const float4 *__restrict__ aV, float *__restrict__ aF,
+                                                   const float *__restrict__ aC, float4 *__restrict__ gridG)
+    {
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
+            loadShapes(sh, shapeTable, p0.numShapes);
+        __syncthreads();
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
+            return;
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && si == 0xFFFFu)
+            return;
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const GridGeom &g = p.g;
+        const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
+        const V3 x = v3(xm[i]);
+        const Stencil st = stencilOf(g, x);
+        if (!st.finite)
+            return;
+        float w[3][3], dw[3][3];
+        weights(st.fx, w);
+        weightGrads(st.fx, dw);
+        // forward replay of v' and C'
+        V3 S = v3(0.f, 0.f, 0.f);
+        float T[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            T[e] = 0.f;
+#pragma unroll 1
+        for (int n = 0; n < 27; ++n)
+        {
+            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
+            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+            if (!inGrid(g, ni, nj, nk))
+                continue;
+            const V3 wv = v3(__ldg(&gridV[nodeAddr(g, ni, nj, nk)])) * (w[a][0] * w[b][1] * w[c][2]);
+            S = S + wv;
+            const float o[3] = {(float)a, (float)b, (float)c};
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                T[3 * r + 0] += o[r] * wv.x;
+                T[3 * r + 1] += o[r] * wv.y;
+                T[3 * r + 2] += o[r] * wv.z;
+            }
+        }
+        const float s4 = 4.f * g.invDx * g.dx;
+        const float fxa[3] = {st.fx.x, st.fx.y, st.fx.z};
+        const float Sv[3] = {S.x, S.y, S.z};
+        M3 Cn;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                Cn.m[3 * c + r] = s4 * (T[3 * r + c] - fxa[r] * Sv[c]);
+        const V3 xpre = x + S * p.dt;
+        V3 xc = v3(fminf(fmaxf(xpre.x, g.gmin.x), g.gmax.x), fminf(fmaxf(xpre.y, g.gmin.y), g.gmax.y),
+                   fminf(fmaxf(xpre.z, g.gmin.z), g.gmax.z));
+        // particle push-out, positions before each contact kept for the reverse
+        V3 hitPos[kAdjMaxHits];
+        int hitShape[kAdjMaxHits];
+        int nh = 0;
+        for (int s = 0; s < p.numShapes; ++s)
+        {
+            const ShapeRec &r = shp[s];
+            if (r.gtype == G_LINES || r.gtype == G_ARC)
+                continue;
+            float dist;
+            V3 nrm, lp, gl;
+            if (!adjShapeEval(r, xc, sdf, dist, nrm, lp, gl))
+                continue;
+            if (!(dist < 0.f))
+                continue;
+            if (nh < kAdjMaxHits)
+            {
+                hitPos[nh] = xc;
+                hitShape[nh] = s;
+                ++nh;
+            }
+            xc = xc - nrm * fminf(dist, 0.f);
+        }
+        // ---- reverse
+        const float4 gx4 = aX[i], gv4 = aV[i];
+        float gFo[9], gCo[9], Fp[9];
+        loadAdj9(aF, stride, i, gFo);
+        loadAdj9(aC, stride, i, gCo);
+        loadAdj9(F, stride, i, Fp);
+        // F' = (I + dt C') F: dL/dC' += dt gF' F^T, dL/dF = (I + dt C')^T gF'   (column-major m[3c + r])
+        float gCt[9], gFn[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                float acc = 0.f, acf = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    acc += gFo[3 * k + r] * Fp[3 * k + c];                                      // (gF' F^T)(r,c)
+                    acf += (((k == r) ? 1.f : 0.f) + p.dt * Cn.m[3 * r + k]) * gFo[3 * c + k]; // ((I+dtC')^T gF')(r,c)
+                }
+                gCt[3 * c + r] = gCo[3 * c + r] + p.dt * acc;
+                gFn[3 * c + r] = acf;
+            }
+        V3 gxp = v3(gx4.x, gx4.y, gx4.z);
+        for (int h = nh - 1; h >= 0; --h)
+        {
+            const ShapeRec &r = shp[hitShape[h]];
+            float dist, J[9];
+            V3 nrm, lp, gl;
+            adjShapeEval(r, hitPos[h], sdf, dist, nrm, lp, gl);
+            adjNormalJacobian(r, lp, gl, J);
+            gxp = gxp - nrm * dot(nrm, gxp) - adjJtG(J, gxp) * dist;
+        }
+        if (xpre.x < g.gmin.x || xpre.x > g.gmax.x)
+            gxp.x = 0.f;
+        if (xpre.y < g.gmin.y || xpre.y > g.gmax.y)
+            gxp.y = 0.f;
+        if (xpre.z < g.gmin.z || xpre.z > g.gmax.z)
+            gxp.z = 0.f;
+        V3 gx = gxp;
+        const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + gxp * p.dt;
+        const float k4 = 4.f * g.invDx;
+        const float ddx = g.invDx * g.dx;
+#pragma unroll 1
+        for (int n = 0; n < 27; ++n)
+        {
+            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
+            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+            if (!inGrid(g, ni, nj, nk))
+                continue;
+            const unsigned ad = nodeAddr(g, ni, nj, nk);
+            const V3 Vn = v3(__ldg(&gridV[ad]));
+            const float W = w[a][0] * w[b][1] * w[c][2];
+            const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]);
+            const float d[3] = {((float)a - st.fx.x) * g.dx, ((float)b - st.fx.y) * g.dx, ((float)c - st.fx.z) * g.dx};
+            // gCd_c = sum_r gC'(r,c) d_r ; gCV_r = sum_c gC'(r,c) V_c
+            const V3 gCd = v3(gCt[0] * d[0] + gCt[1] * d[1] + gCt[2] * d[2], gCt[3] * d[0] + gCt[4] * d[1] + gCt[5] * d[2],
+                              gCt[6] * d[0] + gCt[7] * d[1] + gCt[8] * d[2]);
+            const V3 gCV = v3(gCt[0] * Vn.x + gCt[3] * Vn.y + gCt[6] * Vn.z, gCt[1] * Vn.x + gCt[4] * Vn.y + gCt[7] * Vn.z,
+                              gCt[2] * Vn.x + gCt[5] * Vn.y + gCt[8] * Vn.z);
+            const V3 gVn = (gvt + gCd * k4) * W;
+            atomicAdd(&gridG[ad], make_float4(gVn.x, gVn.y, gVn.z, 0.f));
+            const float gW = dot(Vn, gvt) + k4 * dot(gCd, Vn);
+            gx = gx + gWd * (gW * g.invDx) - gCV * (k4 * W * ddx);
+        }
+        aX[i] = make_float4(gx.x, gx.y, gx.z, 0.f);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            aF[k * stride + i] = gFn[k];
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Reverse of the grid update (per touched node): gridG (dL/dV_n) -> (dL/dP_n, dL/dM_n).
+    // Clears gridA for the next replayed P2G.
+    template <bool Multi>
+    __global__ void __launch_bounds__(256) k_adjGridUpdate(const __grid_constant__ StepParams p0, SceneTable sc,
+                                                          const SortHeader *__restrict__ hdr,
+                                                          const unsigned *__restrict__ touchedList,
+                                                          const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                          float4 *__restrict__ gridA, float4 *__restrict__ gridG)
+    {
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
+            loadShapes(sh, shapeTable, p0.numShapes);
+        __syncthreads();
+        const unsigned nT = hdr->numTouchedBlocks;
+        const unsigned perCta = blockDim.x / 64;
+        for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
+        {
+            const unsigned bi = base + threadIdx.x / 64;
+            if (bi >= nT)
+                continue;
+            const unsigned b = touchedList[bi];
+            const StepParams &p = Multi ? sc.params[sceneOfBlock(sc, b)] : p0;
+            const GridGeom &g = p.g;
+            const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
+            const unsigned l = threadIdx.x & 63;
+            const unsigned lb = b - g.blockBase;
+            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            const int i = 4 * bx + (l & 3), j = 4 * by + ((l >> 2) & 3), k = 4 * bz + (l >> 4);
+            if (!inGrid(g, i, j, k))
+                continue;
+            const unsigned a = b * 64u + l;
+            const float4 acc = gridA[a];
+            gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 gg = gridG[a];
+            V3 gv = v3(gg.x, gg.y, gg.z);
+            if (acc.w < p.cutoff)
+            {
+                gridG[a] = make_float4(gv.x, gv.y, gv.z, 0.f); // light node: V = P
+                continue;
+            }
+            const V3 v0 = v3(acc.x / acc.w, acc.y / acc.w, acc.z / acc.w);
+            const V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z) +
+                           v0 * p.dt;
+            // forward contact chain: velocity before each active contact
+            V3 vin[kAdjMaxHits];
+            int hs[kAdjMaxHits];
+            int nh = 0;
+            V3 v = v0;
+            for (int s = 0; s < p.numShapes; ++s)
+            {
+                const ShapeRec &r = shp[s];
+                float dist;
+                V3 nrm, lp, gl;
+                if (!adjShapeEval(r, pos, sdf, dist, nrm, lp, gl))
+                    continue;
+                if (!(dist < r.params0.x))
+                    continue;
+                const V3 wrel = pos - v3(r.pos);
+                const V3 rv = r.kind == S_STATIC ? v3(0.f, 0.f, 0.f) : v3(r.linVel) + cross(v3(r.angVel), wrel);
+                const V3 rel = v - rv;
+                const float vn = dot(rel, nrm);
+                if (vn >= 0.f)
+                    continue;
+                const V3 tang = rel - nrm * vn;
+                const float tn = sqrtf(sq(tang));
+                const float fc = fmaxf(r.params0.z * vn / (tn + kEps), -1.f);
+                if (nh < kAdjMaxHits)
+                {
+                    vin[nh] = v;
+                    hs[nh] = s;
+                    ++nh;
+                }
+                v = (tang + tang * fc) * r.params0.y + rv;
+            }
+            // boundary band
+            if (i < 2 || i > g.n.x - 3)
+                gv.x = 0.f;
+            if (j < 2 || j > g.n.y - 3)
+                gv.y = 0.f;
+            if (k < 2 || k > g.n.z - 3)
+                gv.z = 0.f;
+            V3 gpos = v3(0.f, 0.f, 0.f);
+            for (int h = nh - 1; h >= 0; --h)
+            {
+                const ShapeRec &r = shp[hs[h]];
+                float dist, J[9];
+                V3 nrm, lp, gl;
+                adjShapeEval(r, pos, sdf, dist, nrm, lp, gl);
+                const V3 wrel = pos - v3(r.pos);
+                const V3 rv = r.kind == S_STATIC ? v3(0.f, 0.f, 0.f) : v3(r.linVel) + cross(v3(r.angVel), wrel);
+                const V3 rel = vin[h] - rv;
+                const float vn = dot(rel, nrm);
+                const V3 tang = rel - nrm * vn;
+                const float tn = sqrtf(sq(tang));
+                const float fr = r.params0.z, sticky = r.params0.y;
+                const float arg = fr * vn / (tn + kEps);
+                V3 grel = v3(0.f, 0.f, 0.f), gn = v3(0.f, 0.f, 0.f);
+                if (arg > -1.f)
+                {
+                    const float fc = arg;
+                    V3 gt = gv * (sticky * (1.f + fc));
+                    const float gfc = sticky * dot(tang, gv);
+                    const float den = tn + kEps;
+                    float gvn = gfc * fr / den;
+                    const float gtn = -gfc * fr * vn / (den * den);
+                    if (tn > 0.f)
+                        gt = gt + tang * (gtn / tn);
+                    grel = gt;
+                    gn = gt * (-vn);
+                    gvn -= dot(nrm, gt);
+                    grel = grel + nrm * gvn;
+                    gn = gn + rel * gvn;
+                }
+                const V3 gvr = gv - grel;
+                adjNormalJacobian(r, lp, gl, J);
+                gpos = gpos + adjJtG(J, gn);
+                if (r.kind != S_STATIC)
+                    gpos = gpos + cross(gvr, v3(r.angVel));
+                gv = grel;
+            }
+            const V3 gv0 = gv + gpos * p.dt;
+            const float im = 1.f / acc.w;
+            gridG[a] = make_float4(gv0.x * im, gv0.y * im, gv0.z * im, -dot(gv0, v0) * im);
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Reverse of P2G and of the stress (per particle); completes the adjoint of the substep's input
+    // state and accumulates dL/dlambda, dL/dmu.
+    template <bool Multi>
+    __global__ void __launch_bounds__(128) k_adjP2G(const __grid_constant__ StepParams p0, SceneTable sc,
+                                                   const float4 *__restrict__ xm, const float4 *__restrict__ vel,
+                                                   const unsigned char *__restrict__ mask,
+                                                   const float4 *__restrict__ matParams, const float *__restrict__ F,
+                                                   const float *__restrict__ Cm, const float *__restrict__ V0,
+                                                   unsigned stride, const float4 *__restrict__ gridG,
+                                                   float4 *__restrict__ aX, float4 *__restrict__ aV,
+                                                   float *__restrict__ aF, float *__restrict__ aC,
+                                                   float4 *__restrict__ aMat)
+    {
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
+            return;
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && si == 0xFFFFu)
+            return;
+        const StepParams &p = Multi ? sc.params[si] : p0;
+        const GridGeom &g = p.g;
+        const float4 x4 = xm[i];
+        const float m = x4.w;
+        const Stencil st = stencilOf(g, v3(x4));
+        if (!st.finite)
+            return;
+        float w[3][3], dw[3][3];
+        weights(st.fx, w);
+        weightGrads(st.fx, dw);
+        M3 Fp, Cp;
+        loadM3(F, stride, i, Fp);
+        loadM3(Cm, stride, i, Cp);
+        const float4 mp = matParams[i];
+        const float lam = mp.x, mu = mp.y;
+        const float J = det3(Fp);
+        const float Jc = J < 1e-6f ? 1e-6f : J;
+        const M3 tau = kirchhoffStress(Fp, lam, mu, 1);
+        const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[i];
+        M3 A;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            A.m[e] = tau.m[e] * coef + Cp.m[e] * m;
+        const V3 u = (v3(vel[i]) + v3(p.gravity) * p.dt) * m;
+        V3 gu = v3(0.f, 0.f, 0.f), gx = v3(0.f, 0.f, 0.f);
+        float gA[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            gA[e] = 0.f;
+        const float ddx = g.invDx * g.dx;
+#pragma unroll 1
+        for (int n = 0; n < 27; ++n)
+        {
+            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
+            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+            if (!inGrid(g, ni, nj, nk))
+                continue;
+            const float4 gg = __ldg(&gridG[nodeAddr(g, ni, nj, nk)]);
+            const V3 gP = v3(gg.x, gg.y, gg.z);
+            const float gM = gg.w;
+            const float W = w[a][0] * w[b][1] * w[c][2];
+            const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]);
+            const V3 d = v3(((float)a - st.fx.x) * g.dx, ((float)b - st.fx.y) * g.dx, ((float)c - st.fx.z) * g.dx);
+            const V3 Ad = v3(A.m[0] * d.x + A.m[3] * d.y + A.m[6] * d.z, A.m[1] * d.x + A.m[4] * d.y + A.m[7] * d.z,
+                             A.m[2] * d.x + A.m[5] * d.y + A.m[8] * d.z);
+            const V3 wgP = gP * W;
+            gu = gu + wgP;
+            // gA(r,c) += W gP_r d_c   (column-major [3c + r])
+            gA[0] += wgP.x * d.x; gA[1] += wgP.y * d.x; gA[2] += wgP.z * d.x;
+            gA[3] += wgP.x * d.y; gA[4] += wgP.y * d.y; gA[5] += wgP.z * d.y;
+            gA[6] += wgP.x * d.z; gA[7] += wgP.y * d.z; gA[8] += wgP.z * d.z;
+            const float gW = dot(gP, u + Ad) + gM * m;
+            // gd = W A^T gP
+            const V3 gd = v3(A.m[0] * gP.x + A.m[1] * gP.y + A.m[2] * gP.z, A.m[3] * gP.x + A.m[4] * gP.y + A.m[5] * gP.z,
+                             A.m[6] * gP.x + A.m[7] * gP.y + A.m[8] * gP.z) * W;
+            gx = gx + gWd * (gW * g.invDx) - gd * ddx;
+        }
+        // stress: tau = mu (F F^T - I) + lam log(J) I
+        float gtau[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            gtau[e] = coef * gA[e];
+        float dmu = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                const float bb = Fp.m[r] * Fp.m[c] + Fp.m[3 + r] * Fp.m[3 + c] + Fp.m[6 + r] * Fp.m[6 + c];
+                dmu += gtau[3 * c + r] * (bb - (r == c ? 1.f : 0.f));
+            }
+        const float trg = gtau[0] + gtau[4] + gtau[8];
+        const float dlam = logf(Jc) * trg;
+        // gF = mu (gtau + gtau^T) F + lam tr(gtau) F^-T
+        float gF[9];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                float s = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    s += (gtau[3 * k + r] + gtau[3 * r + k]) * Fp.m[3 * c + k];
+                gF[3 * c + r] = mu * s;
+            }
+        if (J >= 1e-6f)
+        {
+            const M3 Fi = inverse3(Fp);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    gF[3 * c + r] += lam * trg * Fi.m[3 * r + c];
+        }
+        const float4 ax = aX[i];
+        aX[i] = make_float4(ax.x + gx.x, ax.y + gx.y, ax.z + gx.z, 0.f);
+        aV[i] = make_float4(gu.x * m, gu.y * m, gu.z * m, 0.f);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+        {
+            aF[e * stride + i] += gF[e];
+            aC[e * stride + i] = gA[e] * m;
+        }
+        const float4 am = aMat[i];
+        aMat[i] = make_float4(am.x + dlam, am.y + dmu, 0.f, 0.f);
+    }
+
+    __global__ void k_adjAddSeeds(unsigned n, const float4 *__restrict__ seed, float4 *__restrict__ aX)
+    {
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n)
+            return;
+        const float4 s = seed[i], a = aX[i];
+        aX[i] = make_float4(a.x + s.x, a.y + s.y, a.z + s.z, 0.f);
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Host side
+    void Solver::releaseAdjoint()
+    {
+        void *bufs[] = {adjCkpt, adjSeg, aX, aV, aMat, aF, aC, gridG, adjForce, adjTorque};
+        for (void *b : bufs)
+            if (b)
+                cudaFree(b);
+        adjCkpt = adjSeg = nullptr;
+        aX = aV = aMat = nullptr;
+        aF = aC = nullptr;
+        gridG = adjForce = adjTorque = nullptr;
+        adjCkptCap = adjSegCap = 0;
+        adjRecorded = false;
+    }
+
+    // State blob: x|m (float4 n), v (float4 n), F (9 planes of n), C (9 planes of n).
+    int Solver::saveState(unsigned char *dst)
+    {
+        const size_t n = totalParticles();
+        const size_t pitch = (size_t)numMaxParticles * sizeof(float);
+        CRB_CHECK(cudaMemcpyAsync(dst, positionMass, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpyAsync(dst + n * 16, velocity, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpy2DAsync(dst + n * 32, n * sizeof(float), F, pitch, n * sizeof(float), 9,
+                                    cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpy2DAsync(dst + n * 68, n * sizeof(float), Cm, pitch, n * sizeof(float), 9,
+                                    cudaMemcpyDeviceToDevice, stream));
+        return CRB200_OK;
+    }
+
+    int Solver::loadState(const unsigned char *src)
+    {
+        const size_t n = totalParticles();
+        const size_t pitch = (size_t)numMaxParticles * sizeof(float);
+        CRB_CHECK(cudaMemcpyAsync(positionMass, src, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpyAsync(velocity, src + n * 16, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpy2DAsync(F, pitch, src + n * 32, n * sizeof(float), n * sizeof(float), 9,
+                                    cudaMemcpyDeviceToDevice, stream));
+        CRB_CHECK(cudaMemcpy2DAsync(Cm, pitch, src + n * 68, n * sizeof(float), n * sizeof(float), 9,
+                                    cudaMemcpyDeviceToDevice, stream));
+        return CRB200_OK;
+    }
+
+    // What the adjoint differentiates: MLS-MPM, kinematic contact model, Neo-Hookean active
+    // particles, analytic shapes of uniform scale.  Reads the (small) shape table and the particle
+    // material types / mask back to the host once per recording.
+    int Solver::adjointCheck()
+    {
+        if (solverType != CRB200_SOLVER_GPU_MLS)
+        {
+            setLastError("adjoint: only the MLS-MPM solver has an adjoint");
+            return CRB200_ERR_UNSUPPORTED;
+        }
+        for (const StepParams &sp : allParams())
+            if (sp.contactModel != CRB200_CONTACT_KINEMATIC)
+            {
+                setLastError("adjoint: only the kinematic contact model is differentiated");
+                return CRB200_ERR_UNSUPPORTED;
+            }
+        const unsigned n = totalParticles();
+        if (n == 0 || !matType || !activeMask || !matParams)
+        {
+            setLastError("adjoint: no particles, or materials / active mask not bound");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        std::vector<int> types(n);
+        std::vector<unsigned char> msk(n);
+        CRB_CHECK(cudaMemcpyAsync(types.data(), matType, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CRB_CHECK(cudaMemcpyAsync(msk.data(), activeMask, n, cudaMemcpyDeviceToHost, stream));
+        const int nsh = isBatch() ? totalShapes() : numShapes;
+        std::vector<ShapeRec> recs(nsh > 0 ? nsh : 1);
+        if (nsh > 0)
+        {
+            gatherShapes();
+            CRB_LAUNCHED(1);
+            CRB_CHECK(cudaMemcpyAsync(recs.data(), shapeTable, nsh * sizeof(ShapeRec), cudaMemcpyDeviceToHost, stream));
+        }
+        CRB_CHECK(cudaStreamSynchronize(stream));
+        std::vector<unsigned short> owner;
+        if (isBatch())
+        {
+            owner.resize(n);
+            CRB_CHECK(cudaMemcpy(owner.data(), dParticleScene, n * sizeof(unsigned short), cudaMemcpyDeviceToHost));
+        }
+        for (unsigned q = 0; q < n; ++q)
+        {
+            if (isBatch() && owner[q] == 0xFFFF)
+                continue;
+            if (!msk[q] || types[q] != CRB200_MATERIAL_NEOHOOKEAN)
+            {
+                setLastError("adjoint: every particle must be active and Neo-Hookean");
+                return CRB200_ERR_UNSUPPORTED;
+            }
+        }
+        for (int q = 0; q < nsh; ++q)
+        {
+            const ShapeRec &r = recs[q];
+            if (r.gtype != G_BOX && r.gtype != G_SPHERE && r.gtype != G_PLANE && r.gtype != G_CAPSULE)
+            {
+                setLastError("adjoint: only box, sphere, plane and capsule shapes are differentiated");
+                return CRB200_ERR_UNSUPPORTED;
+            }
+            if (!(r.invScale.x == r.invScale.y && r.invScale.y == r.invScale.z))
+            {
+                setLastError("adjoint: shapes must have uniform scale");
+                return CRB200_ERR_UNSUPPORTED;
+            }
+        }
+        return CRB200_OK;
+    }
+
+    int Solver::adjointRecord(int T, int K, const int *caps, int nc, float4 *capturedX)
+    {
+        if (!initialized)
+        {
+            setLastError("adjoint: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        int r = adjointCheck();
+        if (r != CRB200_OK)
+            return r;
+        const unsigned n = totalParticles();
+        const size_t sb = stateBytes();
+        const int nck = T / K + 2; // checkpoints at 0, K, 2K, ... and the final state
+        if ((size_t)nck * sb > adjCkptCap)
+        {
+            if (adjCkpt)
+                cudaFree(adjCkpt);
+            adjCkpt = nullptr;
+            adjCkptCap = 0;
+            CRB_CHECK(cudaMalloc(&adjCkpt, (size_t)nck * sb));
+            adjCkptCap = (size_t)nck * sb;
+        }
+        adjSubsteps = T;
+        adjInterval = K;
+        adjCaptures.assign(caps, caps + nc);
+        adjRecorded = false;
+        if ((r = saveState(adjCkpt)) != CRB200_OK)
+            return r;
+        int t = 0, c = 0;
+        while (t < T)
+        {
+            int next = std::min(T, (t / K + 1) * K);
+            if (c < nc)
+                next = std::min(next, adjCaptures[c]);
+            if ((r = stepMany(next - t)) != CRB200_OK)
+                return r;
+            t = next;
+            if (c < nc && adjCaptures[c] == t)
+            {
+                CRB_CHECK(cudaMemcpyAsync(capturedX + (size_t)c * n, positionMass, n * sizeof(float4),
+                                          cudaMemcpyDeviceToDevice, stream));
+                ++c;
+            }
+            if (t % K == 0 && t < T)
+                if ((r = saveState(adjCkpt + (size_t)(t / K) * sb)) != CRB200_OK)
+                    return r;
+        }
+        if ((r = saveState(adjCkpt + (size_t)(nck - 1) * sb)) != CRB200_OK)
+            return r;
+        adjRecorded = true;
+        return CRB200_OK;
+    }
+
+    template <bool Multi>
+    int Solver::adjointSubstep()
+    {
+        int r = launchStepT<Multi>(true); // replay: gridA = (P, M), gridV = V
+        if (r != CRB200_OK)
+            return r;
+        const StepParams p = params();
+        const SceneTable sc = sceneTable();
+        const unsigned pg = (sc.numParticles + 127) / 128;
+        const SdfPtrs sp{reinterpret_cast<const int4 *>(sdf.dimension), reinterpret_cast<const float4 *>(sdf.lowerBoundCellSize),
+                         reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
+        const unsigned stride = (unsigned)numMaxParticles;
+        CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
+        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, gridV, aX, aV,
+                                                aF, aC, gridG);
+        k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridG);
+        k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, matParams, F, Cm, V0, stride,
+                                                gridG, aX, aV, aF, aC, aMat);
+        CRB_LAUNCHED(3);
+        return CRB200_OK;
+    }
+
+    int Solver::adjointBackward(const float4 *gradX, float4 *gradV0, float4 *gradMat, float4 *gradX0)
+    {
+        if (!adjRecorded)
+        {
+            setLastError("adjoint: no recorded trajectory (call AdjointRecord first)");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        const unsigned n = totalParticles();
+        const size_t sb = stateBytes();
+        const int T = adjSubsteps, K = adjInterval;
+        const int nck = T / K + 2;
+        const size_t nodes = (size_t)totalBlocks * 64;
+        if (!aX)
+        {
+            const size_t nm = (size_t)numMaxParticles;
+            CRB_CHECK(cudaMalloc(&aX, nm * sizeof(float4)));
+            CRB_CHECK(cudaMalloc(&aV, nm * sizeof(float4)));
+            CRB_CHECK(cudaMalloc(&aMat, nm * sizeof(float4)));
+            CRB_CHECK(cudaMalloc(&aF, 9 * nm * sizeof(float)));
+            CRB_CHECK(cudaMalloc(&aC, 9 * nm * sizeof(float)));
+            CRB_CHECK(cudaMalloc(&gridG, nodes * sizeof(float4)));
+            const int ns = std::max(shapes.size, 1);
+            CRB_CHECK(cudaMalloc(&adjForce, ns * sizeof(float4)));
+            CRB_CHECK(cudaMalloc(&adjTorque, ns * sizeof(float4)));
+        }
+        if ((size_t)K * sb > adjSegCap)
+        {
+            if (adjSeg)
+                cudaFree(adjSeg);
+            adjSeg = nullptr;
+            adjSegCap = 0;
+            CRB_CHECK(cudaMalloc(&adjSeg, (size_t)K * sb));
+            adjSegCap = (size_t)K * sb;
+        }
+        const size_t nm = (size_t)numMaxParticles;
+        CRB_CHECK(cudaMemsetAsync(aX, 0, nm * sizeof(float4), stream));
+        CRB_CHECK(cudaMemsetAsync(aV, 0, nm * sizeof(float4), stream));
+        CRB_CHECK(cudaMemsetAsync(aMat, 0, nm * sizeof(float4), stream));
+        CRB_CHECK(cudaMemsetAsync(aF, 0, 9 * nm * sizeof(float), stream));
+        CRB_CHECK(cudaMemsetAsync(aC, 0, 9 * nm * sizeof(float), stream));
+        const unsigned pg = (n + 127) / 128;
+        int c = (int)adjCaptures.size() - 1;
+        int r = runBackward(gradX, n, pg, sb, T, K, c);
+        adjReplay = false;
+        if (r != CRB200_OK)
+            return r;
+        // leave the solver in the recorded final state
+        if ((r = loadState(adjCkpt + (size_t)(nck - 1) * sb)) != CRB200_OK)
+            return r;
+        if (gradV0)
+            CRB_CHECK(cudaMemcpyAsync(gradV0, aV, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        if (gradMat)
+            CRB_CHECK(cudaMemcpyAsync(gradMat, aMat, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        if (gradX0)
+            CRB_CHECK(cudaMemcpyAsync(gradX0, aX, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+        return CRB200_OK;
+    }
+
+    int Solver::runBackward(const float4 *gradX, unsigned n, unsigned pg, size_t sb, int T, int K, int c)
+    {
+        int r;
+        adjReplay = true;
+        for (int seg = (T - 1) / K; seg >= 0; --seg)
+        {
+            const int t0 = seg * K, t1 = std::min(T, t0 + K);
+            // replay the segment's inputs s_t0 .. s_(t1-1)
+            if ((r = loadState(adjCkpt + (size_t)seg * sb)) != CRB200_OK)
+                return r;
+            for (int t = t0; t < t1; ++t)
+            {
+                if ((r = saveState(adjSeg + (size_t)(t - t0) * sb)) != CRB200_OK)
+                    return r;
+                if (t + 1 < t1 && (r = launchStep()) != CRB200_OK)
+                    return r;
+            }
+            for (int t = t1; t > t0; --t)
+            {
+                while (c >= 0 && adjCaptures[c] == t)
+                {
+                    k_adjAddSeeds<<<pg, 128, 0, stream>>>(n, gradX + (size_t)c * n, aX);
+                    CRB_LAUNCHED(1);
+                    --c;
+                }
+                if ((r = loadState(adjSeg + (size_t)(t - 1 - t0) * sb)) != CRB200_OK)
+                    return r;
+                r = isBatch() ? adjointSubstep<true>() : adjointSubstep<false>();
+                if (r != CRB200_OK)
+                    return r;
+            }
+        }
+        return CRB200_OK;
+    }
+} // namespace crb200

@@ -558,6 +558,36 @@ extern "C"
                           outSubsteps);
     }
 
+    CRB200_API int CrB200SolverAdjointRecord(CrB200SolverHandle solver, int numSubsteps, int checkpointInterval,
+                                             int numCaptures, const int *captureSubsteps,
+                                             CrB200Float4 *capturedPositions)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (numSubsteps <= 0 || checkpointInterval <= 0)
+            return bad("CrB200SolverAdjointRecord: numSubsteps and checkpointInterval must be positive");
+        if (numCaptures < 0 || (numCaptures > 0 && (!captureSubsteps || !capturedPositions)))
+            return bad("CrB200SolverAdjointRecord: captures need a substep list and an output buffer");
+        for (int i = 0; i < numCaptures; ++i)
+        {
+            const int t = captureSubsteps[i];
+            if (t < 1 || t > numSubsteps || (i > 0 && t <= captureSubsteps[i - 1]))
+                return bad("CrB200SolverAdjointRecord: capture substeps must increase strictly within [1, numSubsteps]");
+        }
+        return s->adjointRecord(numSubsteps, checkpointInterval, captureSubsteps, numCaptures,
+                                reinterpret_cast<float4 *>(capturedPositions));
+    }
+
+    CRB200_API int CrB200SolverAdjointBackward(CrB200SolverHandle solver, const CrB200Float4 *gradPositions,
+                                               CrB200Float4 *gradVelocity, CrB200Float4 *gradMaterial,
+                                               CrB200Float4 *gradPosition)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (!gradPositions && !s->adjCaptures.empty())
+            return bad("CrB200SolverAdjointBackward: null gradPositions");
+        return s->adjointBackward(reinterpret_cast<const float4 *>(gradPositions), reinterpret_cast<float4 *>(gradVelocity),
+                                  reinterpret_cast<float4 *>(gradMaterial), reinterpret_cast<float4 *>(gradPosition));
+    }
+
     CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[CRB200_NUM_PHASES],
                                              int *outSubsteps, int reset)
     {

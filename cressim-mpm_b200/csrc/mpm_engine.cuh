@@ -160,7 +160,30 @@ namespace crb200
         int uploadParams();
         int launchStep();   // enqueue one step's kernels
         template <bool Multi>
-        int launchStepT();
+        int launchStepT(bool recompute);
+
+        // adjoint of the MLS-MPM substep (CrB200SolverAdjointRecord / AdjointBackward)
+        int adjointRecord(int numSubsteps, int interval, const int *captures, int numCaptures, float4 *capturedX);
+        int adjointBackward(const float4 *gradX, float4 *gradV0, float4 *gradMat, float4 *gradX0);
+        int runBackward(const float4 *gradX, unsigned n, unsigned pg, size_t sb, int T, int K, int c);
+        void releaseAdjoint();
+        int adjointCheck();
+        int saveState(unsigned char *dst);
+        int loadState(const unsigned char *src);
+        template <bool Multi>
+        int adjointSubstep();
+        size_t stateBytes() const { return (size_t)totalParticles() * (2 * sizeof(float4) + 18 * sizeof(float)); }
+        int adjSubsteps = 0, adjInterval = 0;
+        std::vector<int> adjCaptures;
+        bool adjRecorded = false;
+        bool adjReplay = false;           // substeps replayed by the adjoint send coupling forces to scratch
+        unsigned char *adjCkpt = nullptr; // checkpoint states (every adjInterval substeps and the last)
+        unsigned char *adjSeg = nullptr;  // the states of one segment, recomputed backwards
+        size_t adjCkptCap = 0, adjSegCap = 0;
+        float4 *aX = nullptr, *aV = nullptr, *aMat = nullptr; // adjoint of x, v; d/d(lambda, mu)
+        float *aF = nullptr, *aC = nullptr;                   // adjoint of F, C (planes of stride numMaxParticles)
+        float4 *gridG = nullptr;                               // adjoint of the grid velocity / momentum and mass
+        float4 *adjForce = nullptr, *adjTorque = nullptr;      // coupling output of recomputed substeps
         int sortParticles(const StepParams &p, bool ignoreMask);
         void gatherShapes();
     };

@@ -435,7 +435,7 @@ namespace crb200
                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                         float4 *__restrict__ gridA, float4 *__restrict__ gridF,
                                                         float4 *__restrict__ gridV, float4 *coupleForce,
-                                                        float4 *coupleTorque)
+                                                        float4 *coupleTorque, bool clearA)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         if (!Multi && p0.numShapes > 0)
@@ -461,7 +461,8 @@ namespace crb200
                 continue;
             const unsigned a = b * 64u + l;
             float4 acc = gridA[a];
-            gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (clearA)
+                gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
             float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
             if (withForce)
             {
@@ -1076,6 +1077,7 @@ namespace crb200
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
+        releaseAdjoint();
     }
 
     StepParams Solver::params() const
@@ -1205,12 +1207,14 @@ namespace crb200
     int Solver::launchStep()
     {
         if (isBatch())
-            return launchStepT<true>();
-        return launchStepT<false>();
+            return launchStepT<true>(false);
+        return launchStepT<false>(false);
     }
 
+    // recompute: the adjoint's forward replay of one MLS substep up to the grid update, which
+    // keeps the P2G grid (momentum, mass) in gridA and sends coupling forces to scratch.
     template <bool Multi>
-    int Solver::launchStepT()
+    int Solver::launchStepT(bool recompute)
     {
         if (!Multi && numShapes > kMaxShapes)
         {
@@ -1273,7 +1277,8 @@ namespace crb200
         };
         auto update = [&]() -> int {
             k_gridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV,
-                                                             cf, ct);
+                                                             (recompute || adjReplay) ? adjForce : cf,
+                                                             (recompute || adjReplay) ? adjTorque : ct, !recompute);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1294,6 +1299,8 @@ namespace crb200
             if ((r = p2g(M0{})) != CRB200_OK) return r;
             markPhase(2);
             if ((r = update()) != CRB200_OK) return r;
+            if (recompute)
+                return CRB200_OK;
             markPhase(3);
             if ((r = g2p(M0{})) != CRB200_OK) return r;
         }
@@ -1476,3 +1483,5 @@ namespace crb200
         return CRB200_OK;
     }
 } // namespace crb200
+
+#include "adjoint.cuh"

@@ -304,6 +304,34 @@ CRB200_API int CrB200BatchCreate(int solverType, int numScenes, const CrB200Batc
                                  CrB200SolverHandle *outSolver);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Adjoint of the MLS-MPM substep (no counterpart in the reference: it has no gradient path)   */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Run numSubsteps forward from the solver's current state and record the trajectory for
+ * CrB200SolverAdjointBackward: the state (x, v, F, C) is kept every checkpointInterval substeps
+ * (device memory, 104 bytes per particle per checkpoint) and the rest is recomputed backwards.
+ * captureSubsteps (host, numCaptures entries, strictly increasing in [1, numSubsteps]) lists the
+ * substeps whose positions are copied, as float4 (x, y, z, m), into capturedPositions (device,
+ * numCaptures x numParticles entries, capture-major).  The solver is left in the final state.
+ * Differentiated: the MLS-MPM solver, Neo-Hookean active particles, the kinematic contact model,
+ * box / sphere / plane / capsule shapes of uniform scale (anything else is refused with
+ * CRB200_ERR_UNSUPPORTED).  Works on single-scene solvers and batches alike. */
+CRB200_API int CrB200SolverAdjointRecord(CrB200SolverHandle solver, int numSubsteps, int checkpointInterval,
+                                         int numCaptures, const int *captureSubsteps,
+                                         CrB200Float4 *capturedPositions);
+
+/* Reverse pass over the recorded trajectory.  gradPositions (device, same layout as
+ * capturedPositions; w ignored) holds dL/dx at each captured substep.  Outputs (device, one float4
+ * per particle; any may be NULL): gradVelocity = dL/dv of the recorded initial state,
+ * gradMaterial = (dL/dlambda, dL/dmu, 0, 0) summed over all substeps (lambda, mu = the
+ * particle's params0.x / .y), gradPosition = dL/dx of the initial state with the rest volume V0
+ * held fixed.  Gradients with respect to Young's modulus and Poisson's ratio follow by the chain
+ * rule through lambda(E, nu), mu(E, nu).  Leaves the solver in the recorded final state. */
+CRB200_API int CrB200SolverAdjointBackward(CrB200SolverHandle solver, const CrB200Float4 *gradPositions,
+                                           CrB200Float4 *gradVelocity, CrB200Float4 *gradMaterial,
+                                           CrB200Float4 *gradPosition);
+
+/* ------------------------------------------------------------------------------------------ */
 /* MLS-MPM substep without allocation (no counterpart in the reference)                        */
 /* ------------------------------------------------------------------------------------------ */
 
