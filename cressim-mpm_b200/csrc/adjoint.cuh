@@ -577,6 +577,9 @@ namespace crb200
 
     int Solver::loadState(const unsigned char *src)
     {
+        int rv = invalidateRecords();
+        if (rv != CRB200_OK)
+            return rv;
         const size_t n = totalParticles();
         const size_t pitch = (size_t)numMaxParticles * sizeof(float);
         CRB_CHECK(cudaMemcpyAsync(positionMass, src, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));

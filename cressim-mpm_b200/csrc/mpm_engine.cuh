@@ -65,7 +65,7 @@ namespace crb200
         unsigned fp64Fallbacks;
         unsigned shapeFlags;
         unsigned touchedNodes;
-        unsigned pad;
+        unsigned recordsValid; // set by G2P when it wrote the next substep's P2G records
     };
 
     class Solver
@@ -169,6 +169,7 @@ namespace crb200
         void releaseAdjoint();
         int adjointCheck();
         int saveState(unsigned char *dst);
+        int invalidateRecords();
         int loadState(const unsigned char *src);
         template <bool Multi>
         int adjointSubstep();

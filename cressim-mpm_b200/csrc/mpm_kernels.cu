@@ -594,14 +594,25 @@ namespace crb200
         return r;
     }
 
+    //    records != nullptr (MLS, one scene): also build the next substep's P2G record of the updated
+    //    particle (what k_record would compute from the stored state) unless a slicer is present,
+    //    and mark the records valid; particles whose new stencil leaves the grid are scattered into
+    //    the (cleared) accumulation grid here, as k_record does.
     template <int Mode, bool Multi>
     __global__ void __launch_bounds__(128, 6) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
                                                  float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
                                                  float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                  const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
-                                                 unsigned *status)
+                                                 unsigned *status, const float4 *__restrict__ matParams,
+                                                 const int *__restrict__ matType, const float *__restrict__ V0,
+                                                 float4 *__restrict__ records, float4 *__restrict__ gridA,
+                                                 SortHeader *hdr)
     {
+        constexpr bool kRecords = Mode == 0 && !Multi;
+        const bool writeRecords = kRecords && records != nullptr && !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER));
+        if (writeRecords && blockIdx.x == 0 && threadIdx.x == 0)
+            hdr->recordsValid = 1u; // read only by later launches
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         if (!Multi && p0.numShapes > 0)
         {
@@ -724,6 +735,33 @@ namespace crb200
             storeM3(Cm, stride, i, Cn);
         if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)))
             atomicOr(status, CRB200_STATUS_NAN_STATE);
+        if (kRecords && writeRecords)
+        {
+            RawParticle raw;
+            raw.x4 = make_float4(xn.x, xn.y, xn.z, x4.w);
+            raw.v4 = make_float4(vn.x, vn.y, vn.z, 0.f);
+            raw.mp = matParams[i];
+            raw.mt = matType[i];
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+            {
+                raw.F[e] = Fp.m[e];
+                raw.C[e] = Cn.m[e];
+            }
+            raw.v0 = V0[i];
+            float rec[kRec];
+            if (!buildRecord<0>(p, i, raw, nullptr, stride, 0u, true, gridA, nullptr, nullptr, rec))
+            {
+#pragma unroll
+                for (int e = 0; e < kRec; ++e)
+                    rec[e] = 0.f;
+            }
+            float4 *out = records + 4ull * i;
+            out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+            out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+            out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
+            out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+        }
     }
 
     // PB-MPM integration (pb_mpm_algorithm.h:363-408).
@@ -1287,7 +1325,8 @@ namespace crb200
             if (!pg)
                 return CRB200_OK;
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
-                                                    sp, gridV, cutMasks, &header->status);
+                                                    sp, gridV, cutMasks, &header->status, matParams, matType, V0,
+                                                    (M == 0 && !Multi) ? records : nullptr, gridA, header);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1397,7 +1436,16 @@ namespace crb200
             setLastError("step: solver not initialized");
             return CRB200_ERR_NOT_INITIALIZED;
         }
-        return launchStep();
+        int r = invalidateRecords();
+        return r != CRB200_OK ? r : launchStep();
+    }
+
+    // P2G records written by G2P hold for the next substep of the same call only: the caller may
+    // change particle buffers, materials or parameters between calls.
+    int Solver::invalidateRecords()
+    {
+        CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, sizeof(unsigned), stream));
+        return CRB200_OK;
     }
 
     int Solver::stepMany(int n)
@@ -1409,6 +1457,9 @@ namespace crb200
         }
         if (n <= 0)
             return CRB200_OK;
+        int rv = invalidateRecords();
+        if (rv != CRB200_OK)
+            return rv;
         if (stream == nullptr || n < 2 || phaseTiming)
         {
             for (int i = 0; i < n; ++i)

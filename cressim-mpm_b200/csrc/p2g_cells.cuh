@@ -365,9 +365,10 @@ namespace crb200
         }
     }
 
-    // (b) One record per sorted slot, particle-parallel (full occupancy).  Outliers are scattered
-    //     here with global atomics and leave a zero record.  PB-MPM's material constraint writes
-    //     the relaxed C back.
+    // (b) One record per particle (indexed by particle id), particle-parallel over the sorted slots.
+    //     Outliers are scattered here with global atomics and leave a zero record.  PB-MPM's
+    //     material constraint writes the relaxed C back.  Nothing to do when the previous substep's
+    //     G2P already wrote the records (hdr->recordsValid).
     template <int Mode, bool Multi>
     __global__ void __launch_bounds__(128, Mode == 1 ? 4 : 8) k_record(const __grid_constant__ StepParams p0, SceneTable sc,
                                                     const SortHeader *__restrict__ hdr,
@@ -378,6 +379,8 @@ namespace crb200
                                                     const unsigned *__restrict__ cutMasks, float4 *__restrict__ records,
                                                     float4 *__restrict__ gridA, float4 *__restrict__ gridF, unsigned *fp64Count)
     {
+        if (hdr->recordsValid)
+            return;
         const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
         if (j >= hdr->numSorted)
             return;
@@ -395,7 +398,7 @@ namespace crb200
             for (int e = 0; e < kRec; ++e)
                 rec[e] = 0.f;
         }
-        float4 *out = records + 4ull * j;
+        float4 *out = records + 4ull * id;
         out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
         out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
         out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
@@ -502,17 +505,22 @@ namespace crb200
                     acc[n][3] = 0.f;
                 }
                 float nxt[kRec];
+                unsigned nid = cs < runEnd ? sortedIds[start + cs] : 0u;
                 if (cs < runEnd)
-                    loadRecord(records, start + cs, nxt);
+                    loadRecord(records, nid, nxt);
                 for (unsigned q = cs; q < runEnd; ++q)
                 {
                     float rec[kRec];
 #pragma unroll
                     for (int e = 0; e < kRec; ++e)
                         rec[e] = nxt[e];
+                    const unsigned id = nid;
                     if (q + 1 < runEnd)
-                        loadRecord(records, start + q + 1, nxt);
-                    const unsigned msk = slicers ? cutMasks[sortedIds[start + q]] : 0u;
+                    {
+                        nid = sortedIds[start + q + 1];
+                        loadRecord(records, nid, nxt);
+                    }
+                    const unsigned msk = slicers ? cutMasks[id] : 0u;
                     if (msk)
                         accumulateCell<Mode, true>(p, rec, msk, pass, acc);
                     else
@@ -577,7 +585,8 @@ namespace crb200
                     }
                     const unsigned slot = start + sStart[lo] + (unsigned)kCellRun + (kk - sOv[lo]);
                     float rec[kRec];
-                    loadRecord(records, slot, rec);
+                    const unsigned sid = sortedIds[slot];
+                    loadRecord(records, sid, rec);
                     if (rec[3] == 0.f && rec[0] == 0.f && rec[1] == 0.f && rec[2] == 0.f)
                         continue; // zero record (outlier already scattered, or massless)
                     Stencil st;
@@ -586,7 +595,7 @@ namespace crb200
                     st.b[2] = 4 * bz + (lo >> 4);
                     st.fx = v3(rec[13], rec[14], rec[15]);
                     st.finite = true;
-                    const unsigned msk = slicers ? cutMasks[sortedIds[slot]] : 0u;
+                    const unsigned msk = slicers ? cutMasks[sid] : 0u;
                     if (Mode == 2 && pass == 0)
                         scatterGlobal<2>(p, st, rec, 0u, gridA, gridF);
                     else if (Mode == 2)
