@@ -452,8 +452,12 @@ extern "C"
             e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "read sort header");
-        if (keys && s->numActive)
-            e = cudaMemcpyAsync(keys, s->keys, s->numActive * sizeof(unsigned), cudaMemcpyDeviceToDevice, s->stream);
+        if (keys)
+        {
+            const int r = s->copySortKeys(keys);
+            if (r != CRB200_OK)
+                return r;
+        }
         if (e == cudaSuccess && sortedIds && h.numSorted)
             e = cudaMemcpyAsync(sortedIds, s->sortedIds, h.numSorted * sizeof(unsigned), cudaMemcpyDeviceToDevice,
                                 s->stream);

@@ -65,7 +65,7 @@ namespace crb200
         unsigned fp64Fallbacks;
         unsigned shapeFlags;
         unsigned touchedNodes;
-        unsigned recordsValid; // set by G2P when it wrote the next substep's P2G records
+        unsigned recordsValid; // set by G2P when it binned the particles and wrote the next P2G records
     };
 
     class Solver
@@ -83,6 +83,7 @@ namespace crb200
         int stepMany(int n);
         int computeInitialData(unsigned n, const unsigned *indices);
         int fetchResults();
+        int copySortKeys(unsigned *out);
         int advance(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
         int collectPhaseTimes();
 
@@ -149,6 +150,7 @@ namespace crb200
         int p2gCtas = 0;
         int sortCtas = 0;
         int updCtas = 0;
+        int strideCtas = 0;
 
         cudaGraphExec_t graph = nullptr;
         unsigned graphVersion = ~0u;

@@ -182,6 +182,8 @@ namespace crb200
                           const unsigned char *__restrict__ mask, unsigned *__restrict__ keys,
                           unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount, SortHeader *hdr)
     {
+        if (!Multi && hdr->recordsValid)
+            return; // the previous substep's G2P binned the particles (single scene, MLS)
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         const unsigned lane = threadIdx.x & 31;
         const unsigned n = Multi ? sc.numParticles : p.numActive;
@@ -278,7 +280,10 @@ namespace crb200
     }
 
     // Exclusive scan of the tile sums (single CTA) + totals into the header.
-    __global__ void k_scanTiles(uint3 *__restrict__ tileSums, unsigned numTiles, SortHeader *hdr)
+    // A sorted total above the pair buffer's capacity (inconsistent block counts) empties the
+    // block lists and raises CRB200_STATUS_BLOCK_OVERFLOW instead of letting later kernels run
+    // past the buffers.
+    __global__ void k_scanTiles(uint3 *__restrict__ tileSums, unsigned numTiles, SortHeader *hdr, unsigned capacity)
     {
         __shared__ uint3 carry;
         __shared__ uint3 warpTot[32];
@@ -336,10 +341,13 @@ namespace crb200
         }
         if (threadIdx.x == 0)
         {
-            hdr->numSorted = carry.x;
-            hdr->numActiveBlocks = carry.y;
-            hdr->numTouchedBlocks = carry.z;
+            const bool over = carry.x > capacity;
+            hdr->numSorted = over ? 0u : carry.x;
+            hdr->numActiveBlocks = over ? 0u : carry.y;
+            hdr->numTouchedBlocks = over ? 0u : carry.z;
             hdr->touchedNodes = 0;
+            if (over)
+                atomicOr(&hdr->status, CRB200_STATUS_BLOCK_OVERFLOW);
         }
     }
 
@@ -411,7 +419,8 @@ namespace crb200
     // ---------------------------------------------------------------------------------------
     // 4. Scatter (local cell, id) into the block segments.
     __global__ void k_scatter(unsigned numActive, const unsigned *__restrict__ keys, const unsigned *__restrict__ ranks,
-                              const unsigned *__restrict__ blockStart, unsigned long long *__restrict__ pairs)
+                              const unsigned *__restrict__ blockStart, unsigned long long *__restrict__ pairs,
+                              unsigned capacity)
     {
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         if (i >= numActive)
@@ -419,7 +428,9 @@ namespace crb200
         const unsigned key = keys[i];
         if (key == kInvalidKey)
             return;
-        pairs[blockStart[key >> 6] + ranks[i]] = ((unsigned long long)(key & 63u) << 32) | i;
+        const unsigned slot = blockStart[key >> 6] + ranks[i];
+        if (slot < capacity) // always, unless the block counts were inconsistent (flagged by k_scanTiles)
+            pairs[slot] = ((unsigned long long)(key & 63u) << 32) | i;
     }
 
 }
@@ -438,6 +449,9 @@ namespace crb200
                                                         float4 *coupleTorque, bool clearA)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        __shared__ unsigned sTouched;
+        if (threadIdx.x == 0)
+            sTouched = 0;
         if (!Multi && p0.numShapes > 0)
             loadShapes(sh, shapeTable, p0.numShapes);
         __syncthreads();
@@ -470,11 +484,11 @@ namespace crb200
                 gridF[a] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             {
-                // nodes that received mass (roofline bookkeeping), one atomic per warp
+                // nodes that received mass (roofline bookkeeping): a shared counter per CTA
                 const unsigned am = __activemask();
                 const unsigned hit = __ballot_sync(am, acc.w > 0.f);
                 if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1) && hit)
-                    atomicAdd(&const_cast<SortHeader *>(hdr)->touchedNodes, (unsigned)__popc(hit));
+                    atomicAdd(&sTouched, (unsigned)__popc(hit));
             }
             if (acc.w < p.cutoff)
             {
@@ -500,6 +514,9 @@ namespace crb200
                 v.z = 0.f;
             gridV[a] = make_float4(v.x, v.y, v.z, acc.w);
         }
+        __syncthreads();
+        if (threadIdx.x == 0 && sTouched)
+            atomicAdd(&const_cast<SortHeader *>(hdr)->touchedNodes, sTouched);
     }
 
     // 8. G2P in particle order.  Mode 0 MLS (mls_mpm_algorithm.h:296-390), 1 PB
@@ -607,7 +624,8 @@ namespace crb200
                                                  unsigned *status, const float4 *__restrict__ matParams,
                                                  const int *__restrict__ matType, const float *__restrict__ V0,
                                                  float4 *__restrict__ records, float4 *__restrict__ gridA,
-                                                 SortHeader *hdr)
+                                                 SortHeader *hdr, unsigned *__restrict__ keys,
+                                                 unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount)
     {
         constexpr bool kRecords = Mode == 0 && !Multi;
         const bool writeRecords = kRecords && records != nullptr && !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER));
@@ -761,6 +779,28 @@ namespace crb200
             out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
             out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
             out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+            // binning of the new position for the next substep (what k_bin computes); the lanes
+            // still running aggregate their block histogram updates
+            const Stencil sn = stencilOf(g, xn);
+            bool ood = false;
+            unsigned key = kInvalidKey;
+            if (sn.finite)
+                key = cellKey(g, sn, &ood);
+            else
+                ood = true;
+            const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
+            const unsigned am = __activemask();
+            const unsigned lane = threadIdx.x & 31;
+            const unsigned peers = __match_any_sync(am, blk);
+            const int leader = __ffs(peers) - 1;
+            unsigned base = 0;
+            if (blk != kInvalidKey && (int)lane == leader)
+                base = atomicAdd(&blockCount[blk], (unsigned)__popc(peers));
+            base = __shfl_sync(am, base, leader);
+            keys[i] = key;
+            ranks[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+            if (__any_sync(am, ood) && (int)lane == __ffs(am) - 1)
+                atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
         }
     }
 
@@ -910,14 +950,14 @@ namespace crb200
             loadShapes(sh, shapeTable, p0.numShapes);
             __syncthreads();
         }
-        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= (Multi ? sc.numParticles : p0.numActive))
-            return;
+        const unsigned nP = Multi ? sc.numParticles : p0.numActive;
+        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < nP; i += gridDim.x * blockDim.x)
+        {
         const unsigned si = Multi ? sc.particleScene[i] : 0u;
         if (Multi && (si == 0xFFFFu || !(sc.flags[si] & SF_SLICER)))
         {
             out[i] = 0u;
-            return;
+            continue;
         }
         const StepParams &p = Multi ? sc.params[si] : p0;
         const GridGeom &g = p.g;
@@ -940,6 +980,26 @@ namespace crb200
                     }
         }
         out[i] = msk;
+        }
+    }
+
+    // Cell keys of the most recent sort, rebuilt from its products (the per-particle key array
+    // may already hold the next substep's keys, which G2P writes).
+    __global__ void __launch_bounds__(64) k_sortKeysOut(const SortHeader *__restrict__ hdr,
+                                                        const unsigned *__restrict__ activeList,
+                                                        const unsigned *__restrict__ blockStart,
+                                                        const unsigned *__restrict__ sortedIds,
+                                                        const unsigned char *__restrict__ sortedCell,
+                                                        unsigned *__restrict__ out)
+    {
+        const unsigned nAct = hdr->numActiveBlocks;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
+            for (unsigned t = threadIdx.x; t < cnt; t += 64)
+                out[sortedIds[start + t]] = b * 64u + sortedCell[start + t];
+        }
     }
 
     // ---------------------------------------------------------------------------------------
@@ -1199,6 +1259,7 @@ namespace crb200
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellSort, 64, 0));
         sortCtas = sms * (perSm > 0 ? perSm : 1);
         updCtas = sms * 8;
+        strideCtas = sms * 16; // grid-stride kernels of 128 threads: a full SM each
         initialized = true;
         configVersion++;
         return CRB200_OK;
@@ -1227,13 +1288,14 @@ namespace crb200
         unsigned char *flags = blockFlags;
         k_scanReduce<<<numTiles, kScanThreads, 0, stream>>>(p, sc, totalBlocks, blockCount, flags,
                                                             reinterpret_cast<uint3 *>(tileSums));
-        k_scanTiles<<<1, 1024, 0, stream>>>(reinterpret_cast<uint3 *>(tileSums), numTiles, header);
+        k_scanTiles<<<1, 1024, 0, stream>>>(reinterpret_cast<uint3 *>(tileSums), numTiles, header,
+                                            (unsigned)numMaxParticles);
         k_scanWrite<<<numTiles, kScanThreads, 0, stream>>>(totalBlocks, reinterpret_cast<const uint3 *>(tileSums),
                                                            blockCount, flags, blockStart, activeList, touchedList);
         CRB_LAUNCHED(3);
         if (n > 0)
         {
-            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, blockStart, sortPairs);
+            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, blockStart, sortPairs, (unsigned)numMaxParticles);
             CRB_LAUNCHED(1);
         }
         return CRB200_OK;
@@ -1291,7 +1353,8 @@ namespace crb200
         // iterations, so one evaluation serves every iteration of the step).
         if (numShapes > 0 && !isStd && pg)
         {
-            k_cutMasks<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, shapeTable, sp, cutMasks);
+            k_cutMasks<Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, stream>>>(p, sc, positionMass, activeMask,
+                                                                                     shapeTable, sp, cutMasks);
             CRB_LAUNCHED(1);
         }
         if (nPart > 0)
@@ -1305,7 +1368,7 @@ namespace crb200
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
-            k_record<M, Multi><<<pg, 128, 0, stream>>>(p, sc, header, sortedIds, positionMass, velocity, matParams, matType,
+            k_record<M, Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, stream>>>(p, sc, header, sortedIds, positionMass, velocity, matParams, matType,
                                                         F, Cm, V0, stride, cutMasks, records, gridA, gridF,
                                                         &header->fp64Fallbacks);
             k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, sortedCell,
@@ -1326,7 +1389,8 @@ namespace crb200
                 return CRB200_OK;
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
-                                                    (M == 0 && !Multi) ? records : nullptr, gridA, header);
+                                                    (M == 0 && !Multi) ? records : nullptr, gridA, header, keys, ranks,
+                                                    blockCount);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1440,11 +1504,14 @@ namespace crb200
         return r != CRB200_OK ? r : launchStep();
     }
 
-    // P2G records written by G2P hold for the next substep of the same call only: the caller may
-    // change particle buffers, materials or parameters between calls.
+    // Bins and P2G records written by G2P hold for the next substep of the same call only: the
+    // caller may change particle buffers, materials or parameters between calls.  The block counts
+    // the last G2P of a call accumulated for a substep that did not follow are cleared with the
+    // flag, so that k_bin starts from zero counts.
     int Solver::invalidateRecords()
     {
         CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, sizeof(unsigned), stream));
+        CRB_CHECK(cudaMemsetAsync(blockCount, 0, (totalBlocks + 1) * sizeof(unsigned), stream));
         return CRB200_OK;
     }
 
@@ -1525,6 +1592,17 @@ namespace crb200
         k_initVolume<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA, V0);
         k_initClear<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA);
         CRB_LAUNCHED(3);
+        return CRB200_OK;
+    }
+
+    int Solver::copySortKeys(unsigned *out)
+    {
+        const unsigned n = totalParticles();
+        if (!n)
+            return CRB200_OK;
+        CRB_CHECK(cudaMemsetAsync(out, 0xff, n * sizeof(unsigned), stream));
+        k_sortKeysOut<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortedIds, sortedCell, out);
+        CRB_LAUNCHED(1);
         return CRB200_OK;
     }
 

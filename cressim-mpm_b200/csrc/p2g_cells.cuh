@@ -381,9 +381,9 @@ namespace crb200
     {
         if (hdr->recordsValid)
             return;
-        const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
-        if (j >= hdr->numSorted)
-            return;
+        const unsigned nS = hdr->numSorted;
+        for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < nS; j += gridDim.x * blockDim.x)
+        {
         const unsigned id = sortedIds[j];
         const unsigned si = Multi ? sc.particleScene[id] : 0u; // sorted particles have a scene
         const StepParams &p = Multi ? sc.params[si] : p0;
@@ -403,6 +403,7 @@ namespace crb200
         out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
         out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
         out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+        }
     }
 
     __device__ __forceinline__ void loadRecord(const float4 *__restrict__ records, unsigned j, float rec[kRec])
