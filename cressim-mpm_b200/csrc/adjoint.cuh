@@ -112,6 +112,36 @@ namespace crb200
                   J[2] * g.x + J[5] * g.y + J[8] * g.z);
     }
 
+    // Separable node addresses of a stencil (addr = AX[a] + AY[b] + AZ[c]) and the in-grid bits of
+    // each axis offset (x: bits 0-2, y: 3-5, z: 6-8).
+    struct StencilAddrs
+    {
+        unsigned AX[3], AY[3], AZ[3];
+        unsigned valid;
+        __device__ __forceinline__ bool ok(int a, int b, int c) const
+        {
+            return ((valid >> a) & (valid >> (3 + b)) & (valid >> (6 + c)) & 1u) != 0u;
+        }
+        __device__ __forceinline__ unsigned addr(int a, int b, int c) const { return AX[a] + AY[b] + AZ[c]; }
+    };
+    __device__ __forceinline__ StencilAddrs stencilAddrs(const GridGeom &g, const Stencil &st)
+    {
+        StencilAddrs s;
+        s.valid = 0u;
+#pragma unroll
+        for (int e = 0; e < 3; ++e)
+        {
+            const int xi = st.b[0] + e, yi = st.b[1] + e, zi = st.b[2] + e;
+            s.AX[e] = g.blockBase * 64u + (unsigned)(((xi >> 2) << 6) + (xi & 3));
+            s.AY[e] = (unsigned)(((g.nb.x * (yi >> 2)) << 6) + 4 * (yi & 3));
+            s.AZ[e] = (unsigned)(((g.nb.x * g.nb.y * (zi >> 2)) << 6) + 16 * (zi & 3));
+            s.valid |= ((xi >= 0 && xi < g.n.x) ? 1u : 0u) << e;
+            s.valid |= ((yi >= 0 && yi < g.n.y) ? 1u : 0u) << (3 + e);
+            s.valid |= ((zi >= 0 && zi < g.n.z) ? 1u : 0u) << (6 + e);
+        }
+        return s;
+    }
+
     __device__ __forceinline__ void loadAdj9(const float *planes, unsigned stride, unsigned i, float m[9])
     {
 #pragma unroll
@@ -121,15 +151,19 @@ namespace crb200
 
     // ---------------------------------------------------------------------------------------
     // Reverse of G2P (per particle).  In: adjoint of the substep's output state in aX, aV, aF, aC.
-    // Out: aX, aF hold the G2P part of the adjoint of the input x and F; dL/dV_n is added to gridG.
+    // Out: aX, aF hold the G2P part of the adjoint of the input x and F.  dL/dV_n =
+    // w_n (g_v + 4/dx g_C^T d_n) is affine in the node offset like a P2G contribution, so it is
+    // written as a P2G record (base g_v, matrix 4/dx g_C^T, no mass) that k_accumulate sums into
+    // gridG in cell order; stencils outside the grid are added here with atomics.
     template <bool Multi>
-    __global__ void __launch_bounds__(128) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
+    __global__ void __launch_bounds__(128, 3) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
                                                    const float4 *__restrict__ xm, const unsigned char *__restrict__ mask,
                                                    const float *__restrict__ F, unsigned stride,
                                                    const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                    const float4 *__restrict__ gridV, float4 *__restrict__ aX,
                                                    const float4 *__restrict__ aV, float *__restrict__ aF,
-                                                   const float *__restrict__ aC, float4 *__restrict__ gridG)
+                                                   const float *__restrict__ aC, float4 *__restrict__ gridG,
+                                                   float4 *__restrict__ records)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         if (!Multi && p0.numShapes > 0)
@@ -151,30 +185,68 @@ namespace crb200
         float w[3][3], dw[3][3];
         weights(st.fx, w);
         weightGrads(st.fx, dw);
-        // forward replay of v' and C'
-        V3 S = v3(0.f, 0.f, 0.f);
-        float T[9];
+        // adjoint inputs; g_C' + dt g_F' F^T depends on them only, so the x-gradient moments can be
+        // gathered in the same pass as the forward replay of v' and C'
+        const float4 gx4 = aX[i], gv4 = aV[i];
+        float gFo[9], gCt[9], Fp[9];
+        loadAdj9(aF, stride, i, gFo);
+        loadAdj9(aC, stride, i, gCt);
+        loadAdj9(F, stride, i, Fp);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+            {
+                float acc = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    acc += gFo[3 * k + r] * Fp[3 * k + c]; // (gF' F^T)(r,c)
+                gCt[3 * c + r] += p.dt * acc;
+            }
+        // one pass over the stencil:
+        //   S = sum w V, T[3r + c] = sum o_r w V_c                  (forward v', C')
+        //   G[3k + c] = sum dw/dfx_k V_c, A2_k = sum dw/dfx_k d.(g_C V)  (x-gradient moments)
+        V3 S = v3(0.f, 0.f, 0.f), A2 = v3(0.f, 0.f, 0.f);
+        float T[9], G[9];
 #pragma unroll
         for (int e = 0; e < 9; ++e)
-            T[e] = 0.f;
-#pragma unroll 1
-        for (int n = 0; n < 27; ++n)
         {
-            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
-            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
-            if (!inGrid(g, ni, nj, nk))
-                continue;
-            const V3 wv = v3(__ldg(&gridV[nodeAddr(g, ni, nj, nk)])) * (w[a][0] * w[b][1] * w[c][2]);
-            S = S + wv;
-            const float o[3] = {(float)a, (float)b, (float)c};
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-            {
-                T[3 * r + 0] += o[r] * wv.x;
-                T[3 * r + 1] += o[r] * wv.y;
-                T[3 * r + 2] += o[r] * wv.z;
-            }
+            T[e] = 0.f;
+            G[e] = 0.f;
         }
+        const StencilAddrs sa = stencilAddrs(g, st);
+        const float dfx[3] = {-st.fx.x * g.dx, -st.fx.y * g.dx, -st.fx.z * g.dx};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                {
+                    if (!sa.ok(a, b, c))
+                        continue;
+                    const V3 Vn = v3(__ldg(&gridV[sa.addr(a, b, c)]));
+                    const float wab = w[a][0] * w[b][1];
+                    const float W = wab * w[c][2];
+                    const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], wab * dw[c][2]);
+                    const V3 wv = Vn * W;
+                    S = S + wv;
+                    const float o[3] = {(float)a, (float)b, (float)c};
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+                    {
+                        T[3 * r + 0] += o[r] * wv.x;
+                        T[3 * r + 1] += o[r] * wv.y;
+                        T[3 * r + 2] += o[r] * wv.z;
+                    }
+                    G[0] += gWd.x * Vn.x; G[1] += gWd.x * Vn.y; G[2] += gWd.x * Vn.z;
+                    G[3] += gWd.y * Vn.x; G[4] += gWd.y * Vn.y; G[5] += gWd.y * Vn.z;
+                    G[6] += gWd.z * Vn.x; G[7] += gWd.z * Vn.y; G[8] += gWd.z * Vn.z;
+                    const V3 q = v3(gCt[0] * Vn.x + gCt[3] * Vn.y + gCt[6] * Vn.z, gCt[1] * Vn.x + gCt[4] * Vn.y + gCt[7] * Vn.z,
+                                    gCt[2] * Vn.x + gCt[5] * Vn.y + gCt[8] * Vn.z);
+                    const float e = (o[0] * g.dx + dfx[0]) * q.x + (o[1] * g.dx + dfx[1]) * q.y + (o[2] * g.dx + dfx[2]) * q.z;
+                    A2 = A2 + gWd * e;
+                }
         const float s4 = 4.f * g.invDx * g.dx;
         const float fxa[3] = {st.fx.x, st.fx.y, st.fx.z};
         const float Sv[3] = {S.x, S.y, S.z};
@@ -211,26 +283,17 @@ namespace crb200
             xc = xc - nrm * fminf(dist, 0.f);
         }
         // ---- reverse
-        const float4 gx4 = aX[i], gv4 = aV[i];
-        float gFo[9], gCo[9], Fp[9];
-        loadAdj9(aF, stride, i, gFo);
-        loadAdj9(aC, stride, i, gCo);
-        loadAdj9(F, stride, i, Fp);
-        // F' = (I + dt C') F: dL/dC' += dt gF' F^T, dL/dF = (I + dt C')^T gF'   (column-major m[3c + r])
-        float gCt[9], gFn[9];
+        // F' = (I + dt C') F: dL/dF = (I + dt C')^T gF'   (column-major m[3c + r])
+        float gFn[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
             {
-                float acc = 0.f, acf = 0.f;
+                float acf = 0.f;
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
-                {
-                    acc += gFo[3 * k + r] * Fp[3 * k + c];                                      // (gF' F^T)(r,c)
-                    acf += (((k == r) ? 1.f : 0.f) + p.dt * Cn.m[3 * r + k]) * gFo[3 * c + k]; // ((I+dtC')^T gF')(r,c)
-                }
-                gCt[3 * c + r] = gCo[3 * c + r] + p.dt * acc;
+                    acf += (((k == r) ? 1.f : 0.f) + p.dt * Cn.m[3 * r + k]) * gFo[3 * c + k];
                 gFn[3 * c + r] = acf;
             }
         V3 gxp = v3(gx4.x, gx4.y, gx4.z);
@@ -249,31 +312,67 @@ namespace crb200
             gxp.y = 0.f;
         if (xpre.z < g.gmin.z || xpre.z > g.gmax.z)
             gxp.z = 0.f;
-        V3 gx = gxp;
         const V3 gvt = v3(gv4.x, gv4.y, gv4.z) + gxp * p.dt;
         const float k4 = 4.f * g.invDx;
         const float ddx = g.invDx * g.dx;
-#pragma unroll 1
-        for (int n = 0; n < 27; ++n)
+        // dL/dx = gxp + 1/dx sum_n dw_n (V_n.g_v + 4/dx d_n.(g_C V_n)) - 4/dx (dx/dx) g_C S
+        const V3 Gg = v3(G[0] * gvt.x + G[1] * gvt.y + G[2] * gvt.z, G[3] * gvt.x + G[4] * gvt.y + G[5] * gvt.z,
+                         G[6] * gvt.x + G[7] * gvt.y + G[8] * gvt.z);
+        const V3 gCS = v3(gCt[0] * S.x + gCt[3] * S.y + gCt[6] * S.z, gCt[1] * S.x + gCt[4] * S.y + gCt[7] * S.z,
+                          gCt[2] * S.x + gCt[5] * S.y + gCt[8] * S.z);
+        const V3 gx = gxp + (Gg + A2 * k4) * g.invDx - gCS * (k4 * ddx);
+        const bool inside = st.b[0] >= 0 && st.b[0] <= g.n.x - 2 && st.b[1] >= 0 && st.b[1] <= g.n.y - 2 &&
+                            st.b[2] >= 0 && st.b[2] <= g.n.z - 2;
         {
-            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
-            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
-            if (!inGrid(g, ni, nj, nk))
-                continue;
-            const unsigned ad = nodeAddr(g, ni, nj, nk);
-            const V3 Vn = v3(__ldg(&gridV[ad]));
-            const float W = w[a][0] * w[b][1] * w[c][2];
-            const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]);
-            const float d[3] = {((float)a - st.fx.x) * g.dx, ((float)b - st.fx.y) * g.dx, ((float)c - st.fx.z) * g.dx};
-            // gCd_c = sum_r gC'(r,c) d_r ; gCV_r = sum_c gC'(r,c) V_c
-            const V3 gCd = v3(gCt[0] * d[0] + gCt[1] * d[1] + gCt[2] * d[2], gCt[3] * d[0] + gCt[4] * d[1] + gCt[5] * d[2],
-                              gCt[6] * d[0] + gCt[7] * d[1] + gCt[8] * d[2]);
-            const V3 gCV = v3(gCt[0] * Vn.x + gCt[3] * Vn.y + gCt[6] * Vn.z, gCt[1] * Vn.x + gCt[4] * Vn.y + gCt[7] * Vn.z,
-                              gCt[2] * Vn.x + gCt[5] * Vn.y + gCt[8] * Vn.z);
-            const V3 gVn = (gvt + gCd * k4) * W;
-            atomicAdd(&gridG[ad], make_float4(gVn.x, gVn.y, gVn.z, 0.f));
-            const float gW = dot(Vn, gvt) + k4 * dot(gCd, Vn);
-            gx = gx + gWd * (gW * g.invDx) - gCV * (k4 * W * ddx);
+            // record: u = g_v - A' (fx dx), a_c = dx A'(:, c), A'(r, c) = 4/dx g_C(c, r)
+            float rec[kRec];
+            if (inside)
+            {
+                const float fd[3] = {st.fx.x * g.dx, st.fx.y * g.dx, st.fx.z * g.dx};
+                const float gvv[3] = {gvt.x, gvt.y, gvt.z};
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                {
+                    float sacc = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                    {
+                        const float Ap = k4 * gCt[3 * r + c];
+                        sacc += Ap * fd[c];
+                        rec[4 + 3 * c + r] = Ap * g.dx;
+                    }
+                    rec[r] = gvv[r] - sacc;
+                }
+                rec[3] = 0.f;
+                rec[13] = st.fx.x;
+                rec[14] = st.fx.y;
+                rec[15] = st.fx.z;
+            }
+            else
+            {
+#pragma unroll
+                for (int e = 0; e < kRec; ++e)
+                    rec[e] = 0.f;
+                // stencil crossing the grid edge: its dL/dV_n goes to the grid directly
+#pragma unroll 1
+                for (int n = 0; n < 27; ++n)
+                {
+                    const int a = n / 9, b = (n / 3) % 3, c = n % 3;
+                    if (!sa.ok(a, b, c))
+                        continue;
+                    const float W = w[a][0] * w[b][1] * w[c][2];
+                    const float d[3] = {((float)a - st.fx.x) * g.dx, ((float)b - st.fx.y) * g.dx, ((float)c - st.fx.z) * g.dx};
+                    const V3 gCd = v3(gCt[0] * d[0] + gCt[1] * d[1] + gCt[2] * d[2], gCt[3] * d[0] + gCt[4] * d[1] + gCt[5] * d[2],
+                                      gCt[6] * d[0] + gCt[7] * d[1] + gCt[8] * d[2]);
+                    const V3 gVn = (gvt + gCd * k4) * W;
+                    atomicAdd(&gridG[sa.addr(a, b, c)], make_float4(gVn.x, gVn.y, gVn.z, 0.f));
+                }
+            }
+            float4 *out = records + 4ull * i;
+            out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+            out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+            out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
+            out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
         }
         aX[i] = make_float4(gx.x, gx.y, gx.z, 0.f);
 #pragma unroll
@@ -452,39 +551,54 @@ namespace crb200
         for (int e = 0; e < 9; ++e)
             A.m[e] = tau.m[e] * coef + Cp.m[e] * m;
         const V3 u = (v3(vel[i]) + v3(p.gravity) * p.dt) * m;
-        V3 gu = v3(0.f, 0.f, 0.f), gx = v3(0.f, 0.f, 0.f);
-        float gA[9];
+        // node value u + A d_n = u' + sum_c a_c o_c with u' = u - A (fx dx), a_c = dx A(:, c)
+        const V3 fd = v3(st.fx.x * g.dx, st.fx.y * g.dx, st.fx.z * g.dx);
+        const V3 up = u - v3(A.m[0] * fd.x + A.m[3] * fd.y + A.m[6] * fd.z, A.m[1] * fd.x + A.m[4] * fd.y + A.m[7] * fd.z,
+                             A.m[2] * fd.x + A.m[5] * fd.y + A.m[8] * fd.z);
+        const V3 a0 = v3(A.m[0], A.m[1], A.m[2]) * g.dx, a1 = v3(A.m[3], A.m[4], A.m[5]) * g.dx,
+                 a2 = v3(A.m[6], A.m[7], A.m[8]) * g.dx;
+        // one pass: gu = sum w gP, M[3c + r] = sum w gP_r o_c, gs = sum dw/dfx (gP.(u + A d) + gM m)
+        V3 gu = v3(0.f, 0.f, 0.f), gs = v3(0.f, 0.f, 0.f);
+        float Mo[9];
 #pragma unroll
         for (int e = 0; e < 9; ++e)
-            gA[e] = 0.f;
+            Mo[e] = 0.f;
+        const StencilAddrs sa = stencilAddrs(g, st);
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                {
+                    if (!sa.ok(a, b, c))
+                        continue;
+                    const float4 gg = __ldg(&gridG[sa.addr(a, b, c)]);
+                    const V3 gP = v3(gg.x, gg.y, gg.z);
+                    const float wab = w[a][0] * w[b][1];
+                    const float W = wab * w[c][2];
+                    const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], wab * dw[c][2]);
+                    const V3 wgP = gP * W;
+                    gu = gu + wgP;
+                    if (a) { Mo[0] += (float)a * wgP.x; Mo[1] += (float)a * wgP.y; Mo[2] += (float)a * wgP.z; }
+                    if (b) { Mo[3] += (float)b * wgP.x; Mo[4] += (float)b * wgP.y; Mo[5] += (float)b * wgP.z; }
+                    if (c) { Mo[6] += (float)c * wgP.x; Mo[7] += (float)c * wgP.y; Mo[8] += (float)c * wgP.z; }
+                    const V3 val = up + a0 * (float)a + a1 * (float)b + a2 * (float)c;
+                    gs = gs + gWd * (dot(gP, val) + gg.w * m);
+                }
+        // gA(r, c) = sum w gP_r d_c = dx (M(r, c) - gu_r fx_c);  sum_n w A^T gP = A^T gu
         const float ddx = g.invDx * g.dx;
-#pragma unroll 1
-        for (int n = 0; n < 27; ++n)
-        {
-            const int a = n / 9, b = (n / 3) % 3, c = n % 3;
-            const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
-            if (!inGrid(g, ni, nj, nk))
-                continue;
-            const float4 gg = __ldg(&gridG[nodeAddr(g, ni, nj, nk)]);
-            const V3 gP = v3(gg.x, gg.y, gg.z);
-            const float gM = gg.w;
-            const float W = w[a][0] * w[b][1] * w[c][2];
-            const V3 gWd = v3(dw[a][0] * w[b][1] * w[c][2], w[a][0] * dw[b][1] * w[c][2], w[a][0] * w[b][1] * dw[c][2]);
-            const V3 d = v3(((float)a - st.fx.x) * g.dx, ((float)b - st.fx.y) * g.dx, ((float)c - st.fx.z) * g.dx);
-            const V3 Ad = v3(A.m[0] * d.x + A.m[3] * d.y + A.m[6] * d.z, A.m[1] * d.x + A.m[4] * d.y + A.m[7] * d.z,
-                             A.m[2] * d.x + A.m[5] * d.y + A.m[8] * d.z);
-            const V3 wgP = gP * W;
-            gu = gu + wgP;
-            // gA(r,c) += W gP_r d_c   (column-major [3c + r])
-            gA[0] += wgP.x * d.x; gA[1] += wgP.y * d.x; gA[2] += wgP.z * d.x;
-            gA[3] += wgP.x * d.y; gA[4] += wgP.y * d.y; gA[5] += wgP.z * d.y;
-            gA[6] += wgP.x * d.z; gA[7] += wgP.y * d.z; gA[8] += wgP.z * d.z;
-            const float gW = dot(gP, u + Ad) + gM * m;
-            // gd = W A^T gP
-            const V3 gd = v3(A.m[0] * gP.x + A.m[1] * gP.y + A.m[2] * gP.z, A.m[3] * gP.x + A.m[4] * gP.y + A.m[5] * gP.z,
-                             A.m[6] * gP.x + A.m[7] * gP.y + A.m[8] * gP.z) * W;
-            gx = gx + gWd * (gW * g.invDx) - gd * ddx;
-        }
+        float gA[9];
+        const float fxv[3] = {st.fx.x, st.fx.y, st.fx.z};
+        const float guv[3] = {gu.x, gu.y, gu.z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                gA[3 * c + r] = g.dx * (Mo[3 * c + r] - guv[r] * fxv[c]);
+        const V3 AtG = v3(A.m[0] * gu.x + A.m[1] * gu.y + A.m[2] * gu.z, A.m[3] * gu.x + A.m[4] * gu.y + A.m[5] * gu.z,
+                          A.m[6] * gu.x + A.m[7] * gu.y + A.m[8] * gu.z);
+        const V3 gx = gs * g.invDx - AtG * ddx;
         // stress: tau = mu (F F^T - I) + lam log(J) I
         float gtau[9];
 #pragma unroll
@@ -549,6 +663,7 @@ namespace crb200
     // Host side
     void Solver::releaseAdjoint()
     {
+        releaseAdjointGraphs();
         void *bufs[] = {adjCkpt, adjSeg, aX, aV, aMat, aF, aC, gridG, adjForce, adjTorque};
         for (void *b : bufs)
             if (b)
@@ -726,11 +841,13 @@ namespace crb200
         const unsigned stride = (unsigned)numMaxParticles;
         CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
         k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, gridV, aX, aV,
-                                                aF, aC, gridG);
+                                                aF, aC, gridG, records);
+        k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, sortedCell,
+                                                            records, cutMasks, gridG, gridF);
         k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridG);
         k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, matParams, F, Cm, V0, stride,
                                                 gridG, aX, aV, aF, aC, aMat);
-        CRB_LAUNCHED(3);
+        CRB_LAUNCHED(4);
         return CRB200_OK;
     }
 
@@ -792,10 +909,88 @@ namespace crb200
         return CRB200_OK;
     }
 
+    // One CUDA graph per segment slot k: replay[k] = save the state into slot k and run one forward
+    // substep, reverse[k] = load slot k and run one reverse substep.  Built once per configuration
+    // (pointers, parameters, K) and replayed for every segment of every backward pass.
+    int Solver::captureGraph(int which, int k, cudaGraphExec_t *out, int *kernels)
+    {
+        const size_t sb = stateBytes();
+        const uint64_t before = launchCount();
+        CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int r;
+        if (which == 0)
+        {
+            r = saveState(adjSeg + (size_t)k * sb);
+            if (r == CRB200_OK)
+                r = launchStep();
+        }
+        else
+        {
+            r = loadState(adjSeg + (size_t)k * sb);
+            if (r == CRB200_OK)
+                r = isBatch() ? adjointSubstep<true>() : adjointSubstep<false>();
+        }
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        const uint64_t captured = launchCount() - before;
+        noteLaunches((uint64_t)0 - captured);
+        if (r != CRB200_OK)
+        {
+            if (g)
+                cudaGraphDestroy(g);
+            return r;
+        }
+        if (e != cudaSuccess)
+            return cudaFail(e, "adjoint graph capture");
+        e = cudaGraphInstantiate(out, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess)
+            return cudaFail(e, "adjoint graph instantiate");
+        *kernels = (int)captured;
+        return CRB200_OK;
+    }
+
+    void Solver::releaseAdjointGraphs()
+    {
+        for (auto &v : {&adjReplayG, &adjReverseG})
+            for (cudaGraphExec_t gx : *v)
+                if (gx)
+                    cudaGraphExecDestroy(gx);
+        adjReplayG.clear();
+        adjReverseG.clear();
+        adjGraphKernels[0] = adjGraphKernels[1] = 0;
+    }
+
+    int Solver::adjointGraphs(int K)
+    {
+        if ((int)adjReplayG.size() == K && adjGraphVersion == configVersion && adjGraphSeg == adjSeg)
+            return CRB200_OK;
+        releaseAdjointGraphs();
+        adjReplayG.assign(K, nullptr);
+        adjReverseG.assign(K, nullptr);
+        for (int k = 0; k < K; ++k)
+        {
+            int r = captureGraph(0, k, &adjReplayG[k], &adjGraphKernels[0]);
+            if (r == CRB200_OK)
+                r = captureGraph(1, k, &adjReverseG[k], &adjGraphKernels[1]);
+            if (r != CRB200_OK)
+            {
+                releaseAdjointGraphs();
+                return r;
+            }
+        }
+        adjGraphVersion = configVersion;
+        adjGraphSeg = adjSeg;
+        return CRB200_OK;
+    }
+
     int Solver::runBackward(const float4 *gradX, unsigned n, unsigned pg, size_t sb, int T, int K, int c)
     {
         int r;
         adjReplay = true;
+        const bool graphs = stream != nullptr && !phaseTiming;
+        if (graphs && (r = adjointGraphs(K)) != CRB200_OK)
+            return r;
         for (int seg = (T - 1) / K; seg >= 0; --seg)
         {
             const int t0 = seg * K, t1 = std::min(T, t0 + K);
@@ -804,7 +999,14 @@ namespace crb200
                 return r;
             for (int t = t0; t < t1; ++t)
             {
-                if ((r = saveState(adjSeg + (size_t)(t - t0) * sb)) != CRB200_OK)
+                const int k = t - t0;
+                if (t + 1 < t1 && graphs)
+                {
+                    CRB_CHECK(cudaGraphLaunch(adjReplayG[k], stream));
+                    noteLaunches(adjGraphKernels[0]);
+                    continue;
+                }
+                if ((r = saveState(adjSeg + (size_t)k * sb)) != CRB200_OK)
                     return r;
                 if (t + 1 < t1 && (r = launchStep()) != CRB200_OK)
                     return r;
@@ -817,7 +1019,14 @@ namespace crb200
                     CRB_LAUNCHED(1);
                     --c;
                 }
-                if ((r = loadState(adjSeg + (size_t)(t - 1 - t0) * sb)) != CRB200_OK)
+                const int k = t - 1 - t0;
+                if (graphs)
+                {
+                    CRB_CHECK(cudaGraphLaunch(adjReverseG[k], stream));
+                    noteLaunches(adjGraphKernels[1]);
+                    continue;
+                }
+                if ((r = loadState(adjSeg + (size_t)k * sb)) != CRB200_OK)
                     return r;
                 r = isBatch() ? adjointSubstep<true>() : adjointSubstep<false>();
                 if (r != CRB200_OK)

@@ -168,6 +168,13 @@ namespace crb200
         int adjointRecord(int numSubsteps, int interval, const int *captures, int numCaptures, float4 *capturedX);
         int adjointBackward(const float4 *gradX, float4 *gradV0, float4 *gradMat, float4 *gradX0);
         int runBackward(const float4 *gradX, unsigned n, unsigned pg, size_t sb, int T, int K, int c);
+        int captureGraph(int which, int k, cudaGraphExec_t *out, int *kernels);
+        int adjointGraphs(int K);
+        void releaseAdjointGraphs();
+        std::vector<cudaGraphExec_t> adjReplayG, adjReverseG;
+        int adjGraphKernels[2] = {0, 0};
+        unsigned adjGraphVersion = ~0u;
+        unsigned char *adjGraphSeg = nullptr;
         void releaseAdjoint();
         int adjointCheck();
         int saveState(unsigned char *dst);

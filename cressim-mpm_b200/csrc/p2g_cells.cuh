@@ -419,7 +419,7 @@ namespace crb200
     // (c) Cell accumulation: one 64-thread CTA per active block, one thread per cell.
     //     Multi: each active block reads its scene's parameters (block base search).
     template <int Mode, bool Multi>
-    __global__ void __launch_bounds__(64) k_accumulate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
+    __global__ void __launch_bounds__(64, Multi ? 5 : 6) k_accumulate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                        const unsigned *__restrict__ activeList,
                                                        const unsigned *__restrict__ blockStart,
                                                        const unsigned *__restrict__ sortedIds,
@@ -433,6 +433,7 @@ namespace crb200
         __shared__ unsigned sOv[65];
         __shared__ unsigned sWarpTot;
         __shared__ float sTile[2][4 * kTileNodes];
+        __shared__ StepParams sP; // Multi: the current block's scene parameters
 
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
         const int passes = Mode == 2 ? 2 : 1;
@@ -444,7 +445,16 @@ namespace crb200
         {
             const unsigned b = activeList[ab];
             const unsigned si = Multi ? (unsigned)sceneOfBlock(sc, b) : 0u;
-            const StepParams &p = Multi ? sc.params[si] : p0;
+            if (Multi)
+            {
+                // read at the use sites from shared memory rather than held in registers
+                constexpr int words = (int)(sizeof(StepParams) / sizeof(unsigned));
+                static_assert(words <= 64, "StepParams must fit one load per thread");
+                if (tid < words)
+                    reinterpret_cast<unsigned *>(&sP)[tid] = reinterpret_cast<const unsigned *>(&sc.params[si])[tid];
+                __syncthreads();
+            }
+            const StepParams &p = Multi ? sP : p0;
             const GridGeom &g = p.g;
             const bool slicers = Mode <= 1 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
             const unsigned lb = b - g.blockBase;
