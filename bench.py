@@ -145,6 +145,14 @@ def barrier(world):
         dist.barrier()
 
 
+METRICS = {
+    "slab": "particle-substeps/s (MLS-MPM 1.6M p)",
+    "cube": "particle-substeps/s (MLS-MPM 4096-particle cube)",
+    "pb": "particle-steps/s (PB-MPM cutting, 562k p, 20 iterations per step)",
+}
+UNITS = {"slab": "particle-substeps/s", "cube": "particle-substeps/s", "pb": "particle-steps/s"}
+
+
 def make_workload(name):
     from crmpm_b200 import scenes
 
@@ -152,6 +160,10 @@ def make_workload(name):
         return scenes.tissue_slab(), "MLS-MPM tissue slab + rigid probe, 1.6M particles, 121x61x121 grid, dt 1e-4"
     if name == "cube":
         return scenes.cube_drop(), "MLS-MPM elastic cube drop, 4096 particles, 41^3 grid, dt 2e-4"
+    if name == "pb":
+        sc = scenes.pb_cutting()
+        return sc, (f"PB-MPM slab cut by a kinematic quad-slicer blade, {sc.n} particles, 101x51x101 grid, dt 2e-3, "
+                    f"{sc.iterations} solver iterations per step")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -185,13 +197,17 @@ def run_ours(args, rank, world, local):
     cb.build_library()
     dev = f"cuda:{local}"
     torch.cuda.set_device(local)
+    from crmpm_b200 import scenes as scenes_mod
+
     scene, desc = make_workload(args.workload)
     n = scene.n
     ds = cb.DeviceScene(scene, device=dev)
     s = ds.solver
     stream = ds.stream
-    # warm-up (graph capture happens on the first replay)
+    # warm-up (graph capture happens on the first replay), then the launch-shape autotuner
     ds.step(max(args.warmup, 3))
+    tuned = s.autotune(10)
+    ds.step(3)
     ds.sync()
     st = s.grid_stats()
     touched_nodes = st["touched_nodes"]
@@ -216,7 +232,7 @@ def run_ours(args, rank, world, local):
     ms_max = max_over_ranks(ms, world)
     value = world * n * args.steps / (ms_max / 1e3)
     if args.quick:
-        return {"metric": "particle-substeps/s (MLS-MPM 1.6M p)", "value": value, "unit": "particle-substeps/s",
+        return {"metric": METRICS[args.workload], "value": value, "unit": UNITS[args.workload],
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "quick": True, "gpu_launches": int(launches)}
 
@@ -234,6 +250,13 @@ def run_ours(args, rank, world, local):
     dom = max(("p2g", "g2p", "grid_update"), key=lambda k: per_phase[k])
     achieved = alg[dom] / (per_phase[dom] / 1e3) / 1e9
     substep_bytes = 200.0 * n + 64.0 * touched_nodes
+    if scene.solver_type == scenes_mod.SOLVER_PB:
+        # PB-MPM step: per iteration read x, v, F, m and read / write C (136 B / particle) and 64 B per
+        # touched node, plus the integration's 200 B / particle; the phases fold the iterations
+        # together, so the roofline is given for the whole step
+        substep_bytes = scene.iterations * (136.0 * n + 64.0 * touched_nodes) + 200.0 * n
+        dom = "step"
+        achieved = substep_bytes / (ms / 1e3 / args.steps) / 1e9
     substep_gbs = substep_bytes / (ms / 1e3 / args.steps) / 1e9
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "dram_traffic.txt")
@@ -249,9 +272,10 @@ def run_ours(args, rank, world, local):
     frame_dt = float(np.float32(scene.dt) * frame_substeps) * 0.999
     host_pos = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
     host_vel = torch.empty((ds.num_max, 4), dtype=torch.float32, pin_memory=True)
-    probe = scene.shapes.shape_ids[-1]
+    probe = scene.shapes.shape_ids[-1]  # the moving shape (probe or blade), moved along its velocity
     pose_host = torch.empty(4, dtype=torch.float32, pin_memory=True)
     pose_host.copy_(ds.sh["position"][probe].cpu())
+    probe_vel = scene.shapes.lin_vel[probe, :3].astype(np.float64)
     frames = max(3, args.steps // frame_substeps)
     s.advance(frame_dt, host_pos.data_ptr(), host_vel.data_ptr())  # warm-up
     barrier(world)
@@ -259,7 +283,8 @@ def run_ours(args, rank, world, local):
     t0 = time.perf_counter()
     sub_total = 0
     for f_ in range(frames):
-        pose_host[1] -= 0.1 * scene.dt * frame_substeps
+        for d in range(3):
+            pose_host[d] += float(probe_vel[d]) * scene.dt * frame_substeps
         with torch.cuda.stream(stream):
             ds.sh["position"][probe].copy_(pose_host, non_blocking=True)
         sub_total += s.advance(frame_dt, host_pos.data_ptr(), host_vel.data_ptr())
@@ -274,13 +299,13 @@ def run_ours(args, rank, world, local):
         v, done, el = cpu_reference_run(scene, steps=20, warmup=1, budget_s=25.0)
         if v is not None:
             cpu = {"value": v, "unit": "particle-substeps/s", "cores": 1, "kind": "reference",
-                   "sample": f"{done} MLS substeps of the same 1.6M-particle slab ({el:.1f} s) with the reference's "
+                   "sample": f"{done} substeps of the same workload ({scene.n} particles, {el:.1f} s) with the reference's "
                              f"serial CPU solver arithmetic built from its own headers"}
     status = s.status()
     out = {
-        "metric": "particle-substeps/s (MLS-MPM 1.6M p)",
+        "metric": METRICS[args.workload],
         "value": value,
-        "unit": "particle-substeps/s",
+        "unit": UNITS[args.workload],
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -292,7 +317,8 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded jittered particles)",
         "config": {"workload": desc, "particles": n, "grid": list(s.grid_dims()), "dt": scene.dt,
                    "substeps_per_step": 1, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (particle state ~350 MB)", "touched_nodes": touched_nodes},
+                   "l2": "inputs larger than L2 (particle state ~350 MB)", "touched_nodes": touched_nodes,
+                   "autotuned_launch": {"update_ctas_per_sm": tuned[0], "accumulate_x": tuned[1], "sort_x": tuned[2]}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "phase_ms": per_phase, "substep_gbs_algorithmic": substep_gbs,
@@ -327,6 +353,8 @@ def run_batch(args, rank, world, local):
     n = sum(sc.n for sc in sl_all)
     b = cb.DeviceBatch(sl, device=dev)
     b.step(max(args.warmup, 3))
+    tuned = b.solver.autotune(4)
+    b.step(2)
     b.sync()
     touched_nodes = b.solver.grid_stats()["touched_nodes"]
 
@@ -377,7 +405,8 @@ def run_batch(args, rank, world, local):
         "config": {"workload": "256 MLS-MPM scenes, 64^3-cell grids of 0.02 m, 2k-64k particles each (log-uniform), "
                                "plane + sphere SDF per scene, dt 2e-4", "particles": n, "scenes": len(sl),
                    "touched_nodes_rank0": touched_nodes, "l2": "inputs larger than L2 (particle state ~1 GB)",
-                   "parallelism": f"scene shards x{world}", "scenes_rank0": len(sl)},
+                   "parallelism": f"scene shards x{world}", "scenes_rank0": len(sl),
+                   "autotuned_launch": {"update_ctas_per_sm": tuned[0], "accumulate_x": tuned[1], "sort_x": tuned[2]}},
         "one_by_one": {"value": one_value, "unit": "particle-substeps/s", "substeps": k1,
                        "how": "one plain solver per scene, shared stream, CUDA graph per scene"},
         "batch_over_one_by_one": value / one_value,
@@ -474,7 +503,7 @@ def run_reference(args, rank, world):
               f"reference serial CPU solver arithmetic built from its own headers")
     return {
         "impl": "reference",
-        "metric": "particle-substeps/s (MLS-MPM 1.6M p)",
+        "metric": METRICS[args.workload],
         "value": v,
         "unit": "particle-substeps/s",
         "n_gpus": world,
@@ -498,7 +527,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="slab", choices=["slab", "cube", "batch", "adjoint"])
+    ap.add_argument("--workload", default="slab", choices=["slab", "cube", "pb", "batch", "adjoint"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
                     help="timed region only (no phase pass, e2e or CPU baseline): for profiler launch lists")

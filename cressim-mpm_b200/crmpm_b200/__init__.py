@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
         "CrB200BatchCreate": (i, [i, i, vp, i, i, vp, C.POINTER(vp)]),
         "CrB200SolverAdjointRecord": (i, [vp, i, i, i, vp, vp]),
+        "CrB200SolverAutotune": (i, [vp, i, vp]),
         "CrB200SolverAdjointBackward": (i, [vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
@@ -304,6 +305,13 @@ class GpuSolver:
         n = C.c_int()
         check(lib().CrB200SolverGetPhaseTimes(self._h, ms, C.byref(n), int(reset)), "phase_times")
         return list(ms), n.value
+
+    def autotune(self, substeps_per_trial: int = 8):
+        """Pick the fastest launch shapes (CrB200SolverAutotune); returns (update CTAs per SM,
+        accumulation multiple, sort multiple)."""
+        out = (C.c_int * 3)()
+        check(lib().CrB200SolverAutotune(self._h, int(substeps_per_trial), out), "autotune")
+        return tuple(out)
 
     def adjoint_record(self, num_substeps: int, interval: int, captures, captured_ptr: int):
         caps = (C.c_int * max(len(captures), 1))(*[int(t) for t in captures])

@@ -562,6 +562,14 @@ extern "C"
                           outSubsteps);
     }
 
+    CRB200_API int CrB200SolverAutotune(CrB200SolverHandle solver, int substepsPerTrial, int *outChoiceHost)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (substepsPerTrial < 0)
+            return bad("CrB200SolverAutotune: negative substep count");
+        return s->autotune(substepsPerTrial, outChoiceHost);
+    }
+
     CRB200_API int CrB200SolverAdjointRecord(CrB200SolverHandle solver, int numSubsteps, int checkpointInterval,
                                              int numCaptures, const int *captureSubsteps,
                                              CrB200Float4 *capturedPositions)

@@ -486,12 +486,17 @@ namespace crb200
     //       the smooth distance, separating nodes skipped, Coulomb-like friction, drag, rigid
     //       velocity, line/arc tangent restriction, dynamic coupling (kinematic or effective mass).
     //   isParticle = true: positional push-out only (lines and arcs skipped).
+    //   mask: shapes to consider (bit s = shape s); shapes outside it are known not to reach pos.
     template <bool IsParticle>
     __device__ __forceinline__ void rigidContact(V3 &vel, float m, V3 &pos, const ShapeRec *sh, int num, const SdfPtrs &sdf,
-                                                 bool effMass, float4 *coupleForce, float4 *coupleTorque)
+                                                 bool effMass, float4 *coupleForce, float4 *coupleTorque,
+                                                 unsigned long long mask = ~0ull)
     {
-        for (int s = 0; s < num; ++s)
+        unsigned long long left = mask & (num >= 64 ? ~0ull : ((1ull << num) - 1ull));
+        while (left)
         {
+            const int s = __ffsll((long long)left) - 1;
+            left &= left - 1ull;
             const ShapeRec &r = sh[s];
             if (IsParticle && (r.gtype == G_LINES || r.gtype == G_ARC))
                 continue;
@@ -590,6 +595,40 @@ namespace crb200
                 }
             }
             vel = resp;
+        }
+    }
+
+    // Shapes that may reach some point within R of c, decided by the calling warp (lane s tests
+    // shape s, 32 at a time).  The local SDF is 1-Lipschitz in local coordinates, which stretch by
+    // at most max(invScale): a lower bound at c minus max(invScale) R at or above the culling
+    // threshold (cull.x for grid nodes, cull.y for particles) rules the shape out for the whole
+    // ball.  Every lane of the warp must call it.
+    __device__ __forceinline__ void regionShapeMasks(const ShapeRec *sh, int num, V3 c, float R,
+                                                     unsigned long long &nodeMask, unsigned long long &partMask)
+    {
+        nodeMask = 0ull;
+        partMask = 0ull;
+        const int lane = (int)(threadIdx.x & 31);
+        for (int base = 0; base < num; base += 32)
+        {
+            const int s = base + lane;
+            bool keepNode = false, keepPart = false;
+            if (s < num)
+            {
+                const ShapeRec &r = sh[s];
+                keepNode = keepPart = true;
+                if (r.cull.x < kMaxF32 || r.cull.y < kMaxF32)
+                {
+                    const V3 isc = v3(r.invScale);
+                    const V3 lp = mul(qrotInv(r.rot, c - v3(r.pos)), isc);
+                    const float mx = fmaxf(isc.x, fmaxf(isc.y, isc.z));
+                    const float lb = sdfLowerBound(lp, r.gtype, r.gparams) - mx * R;
+                    keepNode = !(r.cull.x < kMaxF32 && lb >= r.cull.x);
+                    keepPart = !(r.cull.y < kMaxF32 && lb >= r.cull.y);
+                }
+            }
+            nodeMask |= (unsigned long long)__ballot_sync(0xffffffffu, keepNode) << base;
+            partMask |= (unsigned long long)__ballot_sync(0xffffffffu, keepPart) << base;
         }
     }
 

@@ -84,6 +84,8 @@ namespace crb200
         int computeInitialData(unsigned n, const unsigned *indices);
         int fetchResults();
         int copySortKeys(unsigned *out);
+        int autotune(int trial, int choice[3]);
+        int p2gBase = 0, sortBase = 0; // occupancy-derived CTA counts the autotuner multiplies
         int advance(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
         int collectPhaseTimes();
 
@@ -139,6 +141,7 @@ namespace crb200
         unsigned *activeList = nullptr, *touchedList = nullptr;
         unsigned *tileSums = nullptr;
         unsigned char *blockFlags = nullptr;
+        unsigned long long *blockShapeMask = nullptr; // shapes that can reach each block's region (particles)
 
         unsigned *cutMasks = nullptr;
         float4 *records = nullptr;        // P2G records in sorted order, 4 float4 per particle

@@ -115,6 +115,42 @@ namespace crb200
         return blk * 64u + (unsigned)((c[0] & 3) + 4 * ((c[1] & 3) + 4 * (c[2] & 3)));
     }
 
+    // The region of grid block (bx, by, bz) that its shape masks cover: nodes 4b .. 4b+3 and
+    // particles whose base cell lies in the block, each moved by up to two cells (cell units
+    // 4b - 2 .. 4b + 6 per axis).
+    struct BlockRegion
+    {
+        V3 lo, hi;
+        __device__ __forceinline__ bool contains(V3 p) const
+        {
+            return p.x >= lo.x && p.x <= hi.x && p.y >= lo.y && p.y <= hi.y && p.z >= lo.z && p.z <= hi.z;
+        }
+    };
+    __device__ __forceinline__ BlockRegion blockRegion(const GridGeom &g, int bx, int by, int bz)
+    {
+        BlockRegion r;
+        r.lo = v3(g.gmin.x + (float)(4 * bx - 2) * g.dx, g.gmin.y + (float)(4 * by - 2) * g.dx,
+                  g.gmin.z + (float)(4 * bz - 2) * g.dx);
+        r.hi = v3(g.gmin.x + (float)(4 * bx + 6) * g.dx, g.gmin.y + (float)(4 * by + 6) * g.dx,
+                  g.gmin.z + (float)(4 * bz + 6) * g.dx);
+        return r;
+    }
+    // bounding ball of a region, its radius padded against rounding
+    __device__ __forceinline__ void regionBall(const BlockRegion &r, V3 &c, float &R)
+    {
+        c = (r.lo + r.hi) * 0.5f;
+        const V3 h = (r.hi - r.lo) * 0.5f;
+        R = sqrtf(sq(h)) * 1.001f + 1e-6f;
+    }
+    // Block of a particle's (clamped) base cell, as the sort bins it.
+    __device__ __forceinline__ unsigned baseBlock(const GridGeom &g, const Stencil &s, int &bx, int &by, int &bz)
+    {
+        bx = min(max(s.b[0], 0), max(g.n.x - 2, 0)) >> 2;
+        by = min(max(s.b[1], 0), max(g.n.y - 2, 0)) >> 2;
+        bz = min(max(s.b[2], 0), max(g.n.z - 2, 0)) >> 2;
+        return g.blockBase + (unsigned)(bx + g.nb.x * (by + g.nb.y * bz));
+    }
+
     __device__ __forceinline__ void loadM3(const float *planes, unsigned stride, unsigned i, M3 &m)
     {
 #pragma unroll
@@ -446,7 +482,8 @@ namespace crb200
                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                         float4 *__restrict__ gridA, float4 *__restrict__ gridF,
                                                         float4 *__restrict__ gridV, float4 *coupleForce,
-                                                        float4 *coupleTorque, bool clearA)
+                                                        float4 *coupleTorque, bool clearA,
+                                                        unsigned long long *__restrict__ blockShapeMask)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
@@ -470,6 +507,20 @@ namespace crb200
             const unsigned l = threadIdx.x & 63;
             const unsigned lb = b - g.blockBase;
             const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+            // shapes that can reach this block's region: one test per shape and warp instead of
+            // one per node, and the particle mask for G2P / PB-MPM integration
+            const BlockRegion region = blockRegion(g, bx, by, bz);
+            unsigned long long nodeMask = ~0ull;
+            if (p.numShapes > 0)
+            {
+                V3 bc;
+                float bR;
+                regionBall(region, bc, bR);
+                unsigned long long partMask;
+                regionShapeMasks(shp, p.numShapes, bc, bR, nodeMask, partMask);
+                if (l == 0)
+                    blockShapeMask[b] = partMask;
+            }
             const int i = 4 * bx + (l & 3), j = 4 * by + ((l >> 2) & 3), k = 4 * bz + (l >> 4);
             if (!inGrid(g, i, j, k))
                 continue;
@@ -505,7 +556,8 @@ namespace crb200
             V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z);
             pos = pos + v * p.dt;
             if (p.numShapes > 0)
-                rigidContact<false>(v, acc.w, pos, shp, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque);
+                rigidContact<false>(v, acc.w, pos, shp, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque,
+                                    region.contains(pos) ? nodeMask : ~0ull);
             if (i < 2 || i > g.n.x - 3)
                 v.x = 0.f;
             if (j < 2 || j > g.n.y - 3)
@@ -625,7 +677,8 @@ namespace crb200
                                                  const int *__restrict__ matType, const float *__restrict__ V0,
                                                  float4 *__restrict__ records, float4 *__restrict__ gridA,
                                                  SortHeader *hdr, unsigned *__restrict__ keys,
-                                                 unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount)
+                                                 unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
+                                                 const unsigned long long *__restrict__ blockShapeMask)
     {
         constexpr bool kRecords = Mode == 0 && !Multi;
         const bool writeRecords = kRecords && records != nullptr && !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER));
@@ -682,13 +735,53 @@ namespace crb200
                     AY[e] = (unsigned)(((g.nb.x * (yi >> 2)) << 6) + 4 * (yi & 3));
                     AZ[e] = (unsigned)(((g.nb.x * g.nb.y * (zi >> 2)) << 6) + 16 * (zi & 3));
                 }
+                if (Mode == 2)
+                {
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
+                    for (int a = 0; a < 3; ++a)
 #pragma unroll
-                    for (int b = 0; b < 3; ++b)
+                        for (int b = 0; b < 3; ++b)
 #pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            g2pNode<Mode>(a, b, c, v3(__ldg(&gridV[AX[a] + AY[b] + AZ[c]])), w, dw, S, T);
+                            for (int c = 0; c < 3; ++c)
+                                g2pNode<Mode>(a, b, c, v3(__ldg(&gridV[AX[a] + AY[b] + AZ[c]])), w, dw, S, T);
+                }
+                else
+                {
+                    // The weight is a product of 1D factors, so v and the offset moments contract
+                    // axis by axis: over c (Z = sum w_c V, Zc = sum c w_c V), then b, then a.
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        V3 Y = v3(0.f, 0.f, 0.f), Yb = v3(0.f, 0.f, 0.f), Yc = v3(0.f, 0.f, 0.f);
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                        {
+                            const unsigned ab = AX[a] + AY[b];
+                            const V3 v0 = v3(__ldg(&gridV[ab + AZ[0]])), v1 = v3(__ldg(&gridV[ab + AZ[1]])),
+                                     v2 = v3(__ldg(&gridV[ab + AZ[2]]));
+                            const V3 Zc = v1 * w[1][2] + v2 * (2.f * w[2][2]);
+                            const V3 Z = v0 * w[0][2] + v1 * w[1][2] + v2 * w[2][2];
+                            Y = Y + Z * w[b][1];
+                            if (b)
+                                Yb = Yb + Z * ((float)b * w[b][1]);
+                            Yc = Yc + Zc * w[b][1];
+                        }
+                        const V3 wY = Y * w[a][0];
+                        S = S + wY;
+                        if (a)
+                        {
+                            T[0] += (float)a * wY.x;
+                            T[1] += (float)a * wY.y;
+                            T[2] += (float)a * wY.z;
+                        }
+                        T[3] += w[a][0] * Yb.x;
+                        T[4] += w[a][0] * Yb.y;
+                        T[5] += w[a][0] * Yb.z;
+                        T[6] += w[a][0] * Yc.x;
+                        T[7] += w[a][0] * Yc.y;
+                        T[8] += w[a][0] * Yc.z;
+                    }
+                }
             }
             else
             {
@@ -739,7 +832,13 @@ namespace crb200
                 fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
         V3 vn = va;
         if (p.numShapes > 0)
-            rigidContact<true>(vn, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr);
+        {
+            int bx, by, bz;
+            const unsigned blk = baseBlock(g, st, bx, by, bz);
+            const bool near = blockRegion(g, bx, by, bz).contains(xn);
+            rigidContact<true>(vn, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr,
+                               near ? blockShapeMask[blk] : ~0ull);
+        }
         M3 Fp, Mu;
         loadM3(F, stride, i, Fp);
 #pragma unroll
@@ -810,7 +909,8 @@ namespace crb200
                                                          float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
                                                          float *__restrict__ F, const float *__restrict__ Cm,
                                                          unsigned stride, const ShapeRec *__restrict__ shapeTable,
-                                                         SdfPtrs sdf, unsigned *status)
+                                                         SdfPtrs sdf, unsigned *status,
+                                                         const unsigned long long *__restrict__ blockShapeMask)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         if (!Multi && p0.numShapes > 0)
@@ -832,7 +932,14 @@ namespace crb200
                 fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
         v = v + v3(p.gravity) * p.dt;
         if (p.numShapes > 0)
-            rigidContact<true>(v, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr);
+        {
+            const Stencil st = stencilOf(g, v3(x4));
+            int bx, by, bz;
+            const unsigned blk = baseBlock(g, st, bx, by, bz);
+            const bool near = st.finite && blockRegion(g, bx, by, bz).contains(xn);
+            rigidContact<true>(v, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr,
+                               near ? blockShapeMask[blk] : ~0ull);
+        }
         M3 Fp, Cp, Mu;
         loadM3(F, stride, i, Fp);
         loadM3(Cm, stride, i, Cp);
@@ -1171,7 +1278,7 @@ namespace crb200
                 cudaEventDestroy(e);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, sortPairs, blockCount, blockStart,
                         activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, sortedCell,
-                        dParams, dParticleScene, dSceneFlags};
+                        dParams, dParticleScene, dSceneFlags, blockShapeMask};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -1221,6 +1328,7 @@ namespace crb200
         CRB_CHECK(cudaMalloc(&touchedList, totalBlocks * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&tileSums, numTiles * sizeof(uint3)));
         CRB_CHECK(cudaMalloc(&blockFlags, totalBlocks));
+        CRB_CHECK(cudaMalloc(&blockShapeMask, totalBlocks * sizeof(unsigned long long)));
         CRB_CHECK(cudaMalloc(&header, sizeof(SortHeader)));
         const int shapeSlots = isBatch() ? std::max(totalShapes(), 1) : kMaxShapes;
         CRB_CHECK(cudaMalloc(&shapeTable, shapeSlots * sizeof(ShapeRec)));
@@ -1379,7 +1487,8 @@ namespace crb200
         auto update = [&]() -> int {
             k_gridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV,
                                                              (recompute || adjReplay) ? adjForce : cf,
-                                                             (recompute || adjReplay) ? adjTorque : ct, !recompute);
+                                                             (recompute || adjReplay) ? adjTorque : ct, !recompute,
+                                                             blockShapeMask);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1390,7 +1499,7 @@ namespace crb200
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
                                                     (M == 0 && !Multi) ? records : nullptr, gridA, header, keys, ranks,
-                                                    blockCount);
+                                                    blockCount, blockShapeMask);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1420,7 +1529,7 @@ namespace crb200
             if (pg)
             {
                 k_pbIntegrate<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride,
-                                                             shapeTable, sp, &header->status);
+                                                             shapeTable, sp, &header->status, blockShapeMask);
                 CRB_LAUNCHED(1);
             }
         }
@@ -1593,6 +1702,99 @@ namespace crb200
         k_initClear<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA);
         CRB_LAUNCHED(3);
         return CRB200_OK;
+    }
+
+    // Launch-shape autotuner: each candidate (grid-update CTAs per SM, accumulation and cell-sort
+    // CTA counts as multiples of their occupancy) runs `trial` substeps from the same saved state,
+    // timed with CUDA events on the solver stream; the fastest stays.  The particle state is
+    // restored afterwards and coupling forces of the trials go to scratch, so the caller's
+    // simulation is unchanged.
+    int Solver::autotune(int trial, int choice[3])
+    {
+        if (!initialized || stream == nullptr)
+        {
+            setLastError("autotune: needs an initialized solver on a non-default stream");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        if (trial <= 0)
+            trial = 8;
+        int dev = 0, sms = 0;
+        CRB_CHECK(cudaGetDevice(&dev));
+        CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int baseP2g = p2gBase > 0 ? p2gBase : p2gCtas, baseSort = sortBase > 0 ? sortBase : sortCtas;
+        p2gBase = baseP2g;
+        sortBase = baseSort;
+        unsigned char *snap = nullptr;
+        CRB_CHECK(cudaMalloc(&snap, stateBytes()));
+        if (!adjForce)
+        {
+            const int ns = std::max(shapes.size, 1);
+            CRB_CHECK(cudaMalloc(&adjForce, ns * sizeof(float4)));
+            CRB_CHECK(cudaMalloc(&adjTorque, ns * sizeof(float4)));
+        }
+        int r = saveState(snap);
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (r == CRB200_OK)
+            r = cudaFail(cudaEventCreate(&e0), "autotune event");
+        if (r == CRB200_OK)
+            r = cudaFail(cudaEventCreate(&e1), "autotune event");
+        const bool replay0 = adjReplay;
+        adjReplay = true;
+        const int upd[3] = {4, 8, 16}, mul[2] = {1, 2};
+        float best = 1e30f;
+        int bestC[3] = {updCtas / std::max(sms, 1), 1, 1};
+        for (int a = 0; a < 3 && r == CRB200_OK; ++a)
+            for (int b = 0; b < 2 && r == CRB200_OK; ++b)
+                for (int c = 0; c < 2 && r == CRB200_OK; ++c)
+                {
+                    updCtas = sms * upd[a];
+                    p2gCtas = baseP2g * mul[b];
+                    sortCtas = baseSort * mul[c];
+                    configVersion++;
+                    if ((r = loadState(snap)) != CRB200_OK || (r = stepMany(2)) != CRB200_OK)
+                        break; // builds the graph
+                    if ((r = loadState(snap)) != CRB200_OK)
+                        break;
+                    if ((r = cudaFail(cudaEventRecord(e0, stream), "autotune event")) != CRB200_OK)
+                        break;
+                    if ((r = stepMany(trial)) != CRB200_OK)
+                        break;
+                    if ((r = cudaFail(cudaEventRecord(e1, stream), "autotune event")) != CRB200_OK)
+                        break;
+                    float ms = 0.f;
+                    if ((r = cudaFail(cudaEventSynchronize(e1), "autotune sync")) != CRB200_OK)
+                        break;
+                    if ((r = cudaFail(cudaEventElapsedTime(&ms, e0, e1), "autotune timing")) != CRB200_OK)
+                        break;
+                    if (ms < best)
+                    {
+                        best = ms;
+                        bestC[0] = upd[a];
+                        bestC[1] = mul[b];
+                        bestC[2] = mul[c];
+                    }
+                }
+        adjReplay = replay0;
+        updCtas = sms * bestC[0];
+        p2gCtas = baseP2g * bestC[1];
+        sortCtas = baseSort * bestC[2];
+        configVersion++;
+        if (r == CRB200_OK)
+            r = loadState(snap);
+        if (r == CRB200_OK)
+            r = cudaFail(cudaStreamSynchronize(stream), "autotune sync");
+        if (e0)
+            cudaEventDestroy(e0);
+        if (e1)
+            cudaEventDestroy(e1);
+        cudaFree(snap);
+        if (choice)
+        {
+            choice[0] = bestC[0];
+            choice[1] = bestC[1];
+            choice[2] = bestC[2];
+        }
+        return r;
     }
 
     int Solver::copySortKeys(unsigned *out)

@@ -266,6 +266,14 @@ CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int 
 CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[CRB200_NUM_PHASES],
                                          int *outSubsteps, int reset);
 
+/* Launch-shape autotuner (no counterpart in the reference): times the candidate CTA counts of
+ * the grid update (4, 8 or 16 per SM), the cell accumulation and the per-block cell sort (1x or 2x
+ * their occupancy) over substepsPerTrial substeps each (0: 8) from the current state, keeps the
+ * fastest and restores the state; coupling forces of the trials are not reported.  Writes the
+ * choice (update CTAs per SM, accumulation multiple, sort multiple) to outChoiceHost[3] if
+ * given.  Needs a non-default solver stream; synchronizes it. */
+CRB200_API int CrB200SolverAutotune(CrB200SolverHandle solver, int substepsPerTrial, int *outChoiceHost);
+
 /* Grid bookkeeping of the most recent substep: particles binned, active blocks, blocks updated,
  * and nodes that received mass (the touched-node count of the roofline byte model). */
 CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4]);
