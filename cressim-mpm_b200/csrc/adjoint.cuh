@@ -736,7 +736,7 @@ namespace crb200
         std::vector<ShapeRec> recs(nsh > 0 ? nsh : 1);
         if (nsh > 0)
         {
-            gatherShapes();
+            gatherShapes(stream);
             CRB_LAUNCHED(1);
             CRB_CHECK(cudaMemcpyAsync(recs.data(), shapeTable, nsh * sizeof(ShapeRec), cudaMemcpyDeviceToHost, stream));
         }

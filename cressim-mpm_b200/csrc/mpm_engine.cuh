@@ -198,7 +198,9 @@ namespace crb200
         float4 *gridG = nullptr;                               // adjoint of the grid velocity / momentum and mass
         float4 *adjForce = nullptr, *adjTorque = nullptr;      // coupling output of recomputed substeps
         int sortParticles(const StepParams &p, bool ignoreMask);
-        void gatherShapes();
+        void gatherShapes(cudaStream_t s);
+        cudaStream_t sideStream = nullptr; // shape gather / cut masks beside the sort chain
+        cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     };
 
     // Grid of one scene (node counts as the reference's solver constructors compute them).

@@ -668,7 +668,7 @@ namespace crb200
     //    and mark the records valid; particles whose new stencil leaves the grid are scattered into
     //    the (cleared) accumulation grid here, as k_record does.
     template <int Mode, bool Multi>
-    __global__ void __launch_bounds__(128, 6) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
+    __global__ void __launch_bounds__(128, (Mode == 0 && !Multi) ? 7 : 6) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
                                                  float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
                                                  float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -1283,6 +1283,12 @@ namespace crb200
             if (b)
                 cudaFree(b);
         releaseAdjoint();
+        if (forkEvent)
+            cudaEventDestroy(forkEvent);
+        if (joinEvent)
+            cudaEventDestroy(joinEvent);
+        if (sideStream)
+            cudaStreamDestroy(sideStream);
     }
 
     StepParams Solver::params() const
@@ -1367,15 +1373,18 @@ namespace crb200
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellSort, 64, 0));
         sortCtas = sms * (perSm > 0 ? perSm : 1);
         updCtas = sms * 8;
+        CRB_CHECK(cudaStreamCreateWithFlags(&sideStream, cudaStreamNonBlocking));
+        CRB_CHECK(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
+        CRB_CHECK(cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming));
         strideCtas = sms * 16; // grid-stride kernels of 128 threads: a full SM each
         initialized = true;
         configVersion++;
         return CRB200_OK;
     }
 
-    void Solver::gatherShapes()
+    void Solver::gatherShapes(cudaStream_t s)
     {
-        k_gatherShapes<<<numScenes(), 64, 0, stream>>>(params(), sceneTable(), shapeIds, shapes, geometries, shapeTable);
+        k_gatherShapes<<<numScenes(), 64, 0, s>>>(params(), sceneTable(), shapeIds, shapes, geometries, shapeTable);
     }
 
     int Solver::sortParticles(const StepParams &p, bool ignoreMask)
@@ -1443,9 +1452,21 @@ namespace crb200
         const SceneTable sc = sceneTable();
         const unsigned nPart = sc.numParticles;
         markPhase(0);
+        const bool isStd = solverType == CRB200_SOLVER_GPU_STANDARD;
+        // The shape gather and the slicer cut masks depend on the shapes and the positions only:
+        // they run on a side stream beside the sort chain and join before P2G (graph branches
+        // when captured).
+        const bool fork = numShapes > 0 && sideStream != nullptr && stream != nullptr && !phaseTiming;
+        cudaStream_t shapeStream = stream;
+        if (fork)
+        {
+            CRB_CHECK(cudaEventRecord(forkEvent, stream));
+            CRB_CHECK(cudaStreamWaitEvent(sideStream, forkEvent, 0));
+            shapeStream = sideStream;
+        }
         if (numShapes > 0)
         {
-            gatherShapes();
+            gatherShapes(shapeStream);
             CRB_LAUNCHED(1);
         }
         const SdfPtrs sp{reinterpret_cast<const int4 *>(sdf.dimension), reinterpret_cast<const float4 *>(sdf.lowerBoundCellSize),
@@ -1453,24 +1474,27 @@ namespace crb200
         float4 *cf = reinterpret_cast<float4 *>(shapes.force), *ct = reinterpret_cast<float4 *>(shapes.torque);
         const unsigned stride = (unsigned)numMaxParticles;
         const unsigned pg = (nPart + 127) / 128;
-        const bool isStd = solverType == CRB200_SOLVER_GPU_STANDARD;
-        int r = sortParticles(p, isStd);
-        if (r != CRB200_OK)
-            return r;
         // Slicer cut masks of this substep's positions (positions do not change across PB-MPM
         // iterations, so one evaluation serves every iteration of the step).
         if (numShapes > 0 && !isStd && pg)
         {
-            k_cutMasks<Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, stream>>>(p, sc, positionMass, activeMask,
-                                                                                     shapeTable, sp, cutMasks);
+            k_cutMasks<Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, shapeStream>>>(p, sc, positionMass, activeMask,
+                                                                                          shapeTable, sp, cutMasks);
             CRB_LAUNCHED(1);
         }
+        if (fork)
+            CRB_CHECK(cudaEventRecord(joinEvent, sideStream));
+        int r = sortParticles(p, isStd);
+        if (r != CRB200_OK)
+            return r;
         if (nPart > 0)
         {
             k_cellSort<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds, sortedCell,
                                                     &header->status);
             CRB_LAUNCHED(1);
         }
+        if (fork)
+            CRB_CHECK(cudaStreamWaitEvent(stream, joinEvent, 0));
         markPhase(1);
         auto p2g = [&](auto mode) -> int {
             constexpr int M = decltype(mode)::value;
