@@ -842,7 +842,7 @@ namespace crb200
         CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
         k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, gridV, aX, aV,
                                                 aF, aC, gridG, records);
-        k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, sortedCell,
+        k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, cellStart,
                                                             records, cutMasks, gridG, gridF);
         k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridG);
         k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, matParams, F, Cm, V0, stride,

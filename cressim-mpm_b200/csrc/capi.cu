@@ -452,15 +452,12 @@ extern "C"
             e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "read sort header");
-        if (keys)
+        if (keys || sortedIds)
         {
-            const int r = s->copySortKeys(keys);
+            const int r = s->copySortState(keys, h.numSorted ? sortedIds : nullptr);
             if (r != CRB200_OK)
                 return r;
         }
-        if (e == cudaSuccess && sortedIds && h.numSorted)
-            e = cudaMemcpyAsync(sortedIds, s->sortedIds, h.numSorted * sizeof(unsigned), cudaMemcpyDeviceToDevice,
-                                s->stream);
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "copy sort state");
         if (outNumSortedHost)

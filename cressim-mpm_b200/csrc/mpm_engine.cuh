@@ -83,7 +83,7 @@ namespace crb200
         int stepMany(int n);
         int computeInitialData(unsigned n, const unsigned *indices);
         int fetchResults();
-        int copySortKeys(unsigned *out);
+        int copySortState(unsigned *keysOut, unsigned *idsOut);
         int autotune(int trial, int choice[3]);
         int p2gBase = 0, sortBase = 0; // occupancy-derived CTA counts the autotuner multiplies
         int advance(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
@@ -136,7 +136,8 @@ namespace crb200
         float4 *gridV = nullptr; // velocity grid
         float4 *gridF = nullptr; // node force (standard MPM)
         unsigned *keys = nullptr, *ranks = nullptr, *sortedIds = nullptr;
-        unsigned long long *sortPairs = nullptr;
+        unsigned *cellCount = nullptr; // particles per cell (binning), cleared by k_cellStarts
+        unsigned *cellStart = nullptr; // absolute first sorted slot of each cell of the active blocks
         unsigned *blockCount = nullptr, *blockStart = nullptr;
         unsigned *activeList = nullptr, *touchedList = nullptr;
         unsigned *tileSums = nullptr;
@@ -145,7 +146,6 @@ namespace crb200
 
         unsigned *cutMasks = nullptr;
         float4 *records = nullptr;        // P2G records in sorted order, 4 float4 per particle
-        unsigned char *sortedCell = nullptr; // cell (0..63 in its block) of each sorted slot
         SortHeader *header = nullptr;
         ShapeRec *shapeTable = nullptr;
         unsigned totalBlocks = 0;

@@ -1,16 +1,20 @@
 // sm_100a kernels of the B200 MPM substep engine and the host Solver that launches them.
 //
 // One substep (MLS-MPM; the reference's GpuMlsMpmSolver::step, gpu_mls_mpm_solver.cu:102-109):
-//   1. gatherShapes   scene shapes -> compact table (shapes may change between substeps)
-//   2. bin            per particle: cell key (block-major), warp-aggregated block histogram
-//   3. scan           block offsets, active-block list, touched-block list (3 kernels)
-//   4. scatter        (local cell, id) pairs into block segments
-//   5. blockSort      canonical order inside each block: by local cell, then particle id
-//   6. p2g            one CTA per active block: particles -> shared-memory 6x6x6 node tile ->
+//   1. gatherShapes   scene shapes -> compact table (shapes may change between substeps); with the
+//                     slicer cut masks on a side stream beside the sort chain
+//   2. bin            per particle: cell key (block-major), rank among its cell's particles, cell
+//                     and block counts (warp-aggregated atomics); done by the previous G2P when
+//                     it can be
+//   3. scan           block offsets, active-block list, touched-block list (3 kernels), then the
+//                     absolute start of every cell of the active blocks
+//   4. scatter        particle ids into their cells' slots (cells contiguous in key order; arrival
+//                     order inside a cell; the canonical order is produced on request)
+//   5. p2g            one CTA per active block: particles -> shared-memory 6x6x6 node tile ->
 //                     one float4 vector atomic per touched node into the accumulation grid
-//   7. gridUpdate     touched blocks only: momentum -> velocity, SDF contact/friction, domain BC,
+//   6. gridUpdate     touched blocks only: momentum -> velocity, SDF contact/friction, domain BC,
 //                     and the accumulation grid is zeroed as it is consumed
-//   8. g2p            particle order: 27-node gather, APIC matrix, advection, push-out, F update
+//   7. g2p            particle order: 27-node gather, APIC matrix, advection, push-out, F update
 // PB-MPM runs 6-8 `iterations` times per step plus an integration kernel (gpu_pb_mpm_solver.cu:
 // 102-113); standard MPM carries a node force tile (gpu_standard_mpm_solver.cu:177-184).
 
@@ -173,6 +177,30 @@ namespace crb200
             d[t] = s[t];
     }
 
+    // Records one binned particle of the calling lanes (active lanes `am`): its key, its rank among
+    // the particles of its cell (arrival order), and the cell and block counts, with one atomic per
+    // group of lanes sharing a cell or a block.
+    __device__ __forceinline__ void binAggregated(unsigned am, unsigned lane, unsigned key, unsigned *__restrict__ blockCount,
+                                                  unsigned *__restrict__ cellCount, unsigned *keyOut, unsigned *rankOut)
+    {
+        const unsigned lt = (1u << lane) - 1u;
+        const unsigned cellPeers = __match_any_sync(am, key);
+        const int cellLeader = __ffs(cellPeers) - 1;
+        unsigned base = 0;
+        if (key != kInvalidKey && (int)lane == cellLeader)
+            base = atomicAdd(&cellCount[key], (unsigned)__popc(cellPeers));
+        base = __shfl_sync(am, base, cellLeader);
+        const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
+        const unsigned blkPeers = __match_any_sync(am, blk);
+        if (blk != kInvalidKey && (int)lane == __ffs(blkPeers) - 1)
+            atomicAdd(&blockCount[blk], (unsigned)__popc(blkPeers));
+        if (keyOut)
+        {
+            *keyOut = key;
+            *rankOut = base + (unsigned)__popc(cellPeers & lt);
+        }
+    }
+
     // Scene of a block (binary search over the scenes' block bases; scene 0 for one scene).
     __device__ __forceinline__ int sceneOfBlock(const SceneTable &sc, unsigned b)
     {
@@ -216,7 +244,8 @@ namespace crb200
     template <bool Multi>
     __global__ void k_bin(const __grid_constant__ StepParams p, SceneTable sc, bool ignoreMask, const float4 *__restrict__ xm,
                           const unsigned char *__restrict__ mask, unsigned *__restrict__ keys,
-                          unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount, SortHeader *hdr)
+                          unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
+                          unsigned *__restrict__ cellCount, SortHeader *hdr)
     {
         if (!Multi && hdr->recordsValid)
             return; // the previous substep's G2P binned the particles (single scene, MLS)
@@ -239,18 +268,7 @@ namespace crb200
                     ood = true;
             }
         }
-        const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
-        const unsigned peers = __match_any_sync(0xffffffffu, blk);
-        const int leader = __ffs(peers) - 1;
-        unsigned base = 0;
-        if (blk != kInvalidKey && (int)lane == leader)
-            base = atomicAdd(&blockCount[blk], (unsigned)__popc(peers));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (i < n)
-        {
-            keys[i] = key;
-            ranks[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
-        }
+        binAggregated(0xffffffffu, lane, key, blockCount, cellCount, i < n ? &keys[i] : nullptr, i < n ? &ranks[i] : nullptr);
         if (__any_sync(0xffffffffu, ood) && lane == 0)
             atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
     }
@@ -455,7 +473,7 @@ namespace crb200
     // ---------------------------------------------------------------------------------------
     // 4. Scatter (local cell, id) into the block segments.
     __global__ void k_scatter(unsigned numActive, const unsigned *__restrict__ keys, const unsigned *__restrict__ ranks,
-                              const unsigned *__restrict__ blockStart, unsigned long long *__restrict__ pairs,
+                              const unsigned *__restrict__ cellStart, unsigned *__restrict__ sortedIds,
                               unsigned capacity)
     {
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -464,9 +482,42 @@ namespace crb200
         const unsigned key = keys[i];
         if (key == kInvalidKey)
             return;
-        const unsigned slot = blockStart[key >> 6] + ranks[i];
+        const unsigned slot = cellStart[key] + ranks[i];
         if (slot < capacity) // always, unless the block counts were inconsistent (flagged by k_scanTiles)
-            pairs[slot] = ((unsigned long long)(key & 63u) << 32) | i;
+            sortedIds[slot] = i;
+    }
+
+    // Absolute start of every cell of the active blocks (one 64-thread CTA per block, one thread per
+    // cell): the block's start plus the exclusive prefix of its cell counts, which are cleared for
+    // the next binning.
+    __global__ void __launch_bounds__(64) k_cellStarts(const SortHeader *__restrict__ hdr,
+                                                       const unsigned *__restrict__ activeList,
+                                                       const unsigned *__restrict__ blockStart,
+                                                       unsigned *__restrict__ cellCount, unsigned *__restrict__ cellStart)
+    {
+        __shared__ unsigned warpTot;
+        const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const unsigned nAct = hdr->numActiveBlocks;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab];
+            const unsigned c = b * 64u + tid;
+            const unsigned v = cellCount[c];
+            cellCount[c] = 0u;
+            unsigned inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= (unsigned)o)
+                    inc += y;
+            }
+            if (tid == 31)
+                warpTot = inc;
+            __syncthreads();
+            cellStart[c] = blockStart[b] + inc - v + (warp ? warpTot : 0u);
+            __syncthreads();
+        }
     }
 
 }
@@ -678,6 +729,7 @@ namespace crb200
                                                  float4 *__restrict__ records, float4 *__restrict__ gridA,
                                                  SortHeader *hdr, unsigned *__restrict__ keys,
                                                  unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
+                                                 unsigned *__restrict__ cellCount,
                                                  const unsigned long long *__restrict__ blockShapeMask)
     {
         constexpr bool kRecords = Mode == 0 && !Multi;
@@ -887,17 +939,9 @@ namespace crb200
                 key = cellKey(g, sn, &ood);
             else
                 ood = true;
-            const unsigned blk = key == kInvalidKey ? kInvalidKey : key >> 6;
             const unsigned am = __activemask();
             const unsigned lane = threadIdx.x & 31;
-            const unsigned peers = __match_any_sync(am, blk);
-            const int leader = __ffs(peers) - 1;
-            unsigned base = 0;
-            if (blk != kInvalidKey && (int)lane == leader)
-                base = atomicAdd(&blockCount[blk], (unsigned)__popc(peers));
-            base = __shfl_sync(am, base, leader);
-            keys[i] = key;
-            ranks[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+            binAggregated(am, lane, key, blockCount, cellCount, &keys[i], &ranks[i]);
             if (__any_sync(am, ood) && (int)lane == __ffs(am) - 1)
                 atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
         }
@@ -1096,18 +1140,37 @@ namespace crb200
                                                         const unsigned *__restrict__ activeList,
                                                         const unsigned *__restrict__ blockStart,
                                                         const unsigned *__restrict__ sortedIds,
-                                                        const unsigned char *__restrict__ sortedCell,
-                                                        unsigned *__restrict__ out)
+                                                        const unsigned *__restrict__ cellStart,
+                                                        unsigned *__restrict__ keysOut, unsigned *__restrict__ idsOut)
     {
+        // keysOut: the key of every sorted particle; idsOut: each cell's ids in increasing order
+        // (the canonical permutation: by key, ties by particle id)
         const unsigned nAct = hdr->numActiveBlocks;
         for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
         {
             const unsigned b = activeList[ab];
-            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            for (unsigned t = threadIdx.x; t < cnt; t += 64)
-                out[sortedIds[start + t]] = b * 64u + sortedCell[start + t];
+            const unsigned c = b * 64u + threadIdx.x;
+            const unsigned cs = cellStart[c], ce = threadIdx.x < 63 ? cellStart[c + 1] : blockStart[b + 1];
+            for (unsigned t = cs; t < ce; ++t)
+            {
+                const unsigned id = sortedIds[t];
+                if (keysOut)
+                    keysOut[id] = c;
+                if (idsOut)
+                {
+                    // insertion into the already written, sorted prefix of this cell
+                    unsigned u = t;
+                    while (u > cs && idsOut[u - 1] > id)
+                    {
+                        idsOut[u] = idsOut[u - 1];
+                        --u;
+                    }
+                    idsOut[u] = id;
+                }
+            }
         }
     }
+
 
     // ---------------------------------------------------------------------------------------
     // Host side
@@ -1276,8 +1339,8 @@ namespace crb200
         for (cudaEvent_t e : phaseEv)
             if (e)
                 cudaEventDestroy(e);
-        void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, sortPairs, blockCount, blockStart,
-                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, sortedCell,
+        void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, cellCount, blockCount, blockStart,
+                        activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, cellStart,
                         dParams, dParticleScene, dSceneFlags, blockShapeMask};
         for (void *b : bufs)
             if (b)
@@ -1327,7 +1390,9 @@ namespace crb200
         CRB_CHECK(cudaMalloc(&keys, n * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&ranks, n * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&sortedIds, n * sizeof(unsigned)));
-        CRB_CHECK(cudaMalloc(&sortPairs, n * sizeof(unsigned long long)));
+        CRB_CHECK(cudaMalloc(&cellCount, (size_t)totalBlocks * 64 * sizeof(unsigned)));
+        CRB_CHECK(cudaMalloc(&cellStart, (size_t)totalBlocks * 64 * sizeof(unsigned)));
+        CRB_CHECK(cudaMemsetAsync(cellCount, 0, (size_t)totalBlocks * 64 * sizeof(unsigned), stream));
         CRB_CHECK(cudaMalloc(&blockCount, (totalBlocks + 1) * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&blockStart, (totalBlocks + 1) * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&activeList, totalBlocks * sizeof(unsigned)));
@@ -1354,7 +1419,6 @@ namespace crb200
         }
         CRB_CHECK(cudaMalloc(&cutMasks, n * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&records, n * 4 * sizeof(float4)));
-        CRB_CHECK(cudaMalloc(&sortedCell, n));
         CRB_CHECK(cudaMemsetAsync(F, 0, 9 * n * sizeof(float), stream));
         CRB_CHECK(cudaMemsetAsync(Cm, 0, 9 * n * sizeof(float), stream));
         CRB_CHECK(cudaMemsetAsync(V0, 0, n * sizeof(float), stream));
@@ -1370,7 +1434,7 @@ namespace crb200
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0, false>, 64, 0));
         p2gCtas = sms * (perSm > 0 ? perSm : 1);
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellSort, 64, 0));
+        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellStarts, 64, 0));
         sortCtas = sms * (perSm > 0 ? perSm : 1);
         updCtas = sms * 8;
         CRB_CHECK(cudaStreamCreateWithFlags(&sideStream, cudaStreamNonBlocking));
@@ -1396,10 +1460,10 @@ namespace crb200
         {
             if (isBatch())
                 k_bin<true><<<pg, 128, 0, stream>>>(p, sc, ignoreMask, positionMass, activeMask, keys, ranks, blockCount,
-                                                    header);
+                                                    cellCount, header);
             else
                 k_bin<false><<<pg, 128, 0, stream>>>(p, sc, ignoreMask, positionMass, activeMask, keys, ranks, blockCount,
-                                                     header);
+                                                     cellCount, header);
             CRB_LAUNCHED(1);
         }
         unsigned char *flags = blockFlags;
@@ -1412,7 +1476,8 @@ namespace crb200
         CRB_LAUNCHED(3);
         if (n > 0)
         {
-            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, blockStart, sortPairs, (unsigned)numMaxParticles);
+            k_cellStarts<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, cellCount, cellStart);
+            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, cellStart, sortedIds, (unsigned)numMaxParticles);
             CRB_LAUNCHED(1);
         }
         return CRB200_OK;
@@ -1487,12 +1552,6 @@ namespace crb200
         int r = sortParticles(p, isStd);
         if (r != CRB200_OK)
             return r;
-        if (nPart > 0)
-        {
-            k_cellSort<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortPairs, sortedIds, sortedCell,
-                                                    &header->status);
-            CRB_LAUNCHED(1);
-        }
         if (fork)
             CRB_CHECK(cudaStreamWaitEvent(stream, joinEvent, 0));
         markPhase(1);
@@ -1503,7 +1562,7 @@ namespace crb200
             k_record<M, Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, stream>>>(p, sc, header, sortedIds, positionMass, velocity, matParams, matType,
                                                         F, Cm, V0, stride, cutMasks, records, gridA, gridF,
                                                         &header->fp64Fallbacks);
-            k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, sortedCell,
+            k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, cellStart,
                                                                 records, cutMasks, gridA, gridF);
             CRB_LAUNCHED(2);
             return CRB200_OK;
@@ -1523,7 +1582,7 @@ namespace crb200
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
                                                     (M == 0 && !Multi) ? records : nullptr, gridA, header, keys, ranks,
-                                                    blockCount, blockShapeMask);
+                                                    blockCount, cellCount, blockShapeMask);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -1645,6 +1704,7 @@ namespace crb200
     {
         CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, sizeof(unsigned), stream));
         CRB_CHECK(cudaMemsetAsync(blockCount, 0, (totalBlocks + 1) * sizeof(unsigned), stream));
+        CRB_CHECK(cudaMemsetAsync(cellCount, 0, (size_t)totalBlocks * 64 * sizeof(unsigned), stream));
         return CRB200_OK;
     }
 
@@ -1821,16 +1881,18 @@ namespace crb200
         return r;
     }
 
-    int Solver::copySortKeys(unsigned *out)
+    int Solver::copySortState(unsigned *keysOut, unsigned *idsOut)
     {
         const unsigned n = totalParticles();
         if (!n)
             return CRB200_OK;
-        CRB_CHECK(cudaMemsetAsync(out, 0xff, n * sizeof(unsigned), stream));
-        k_sortKeysOut<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortedIds, sortedCell, out);
+        if (keysOut)
+            CRB_CHECK(cudaMemsetAsync(keysOut, 0xff, n * sizeof(unsigned), stream));
+        k_sortKeysOut<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortedIds, cellStart, keysOut, idsOut);
         CRB_LAUNCHED(1);
         return CRB200_OK;
     }
+
 
     int Solver::fetchResults()
     {

@@ -1,23 +1,20 @@
 // P2G with one thread per grid cell (included by mpm_kernels.cu).
 //
 // One 64-thread CTA takes one 4x4x4-cell block of the sorted particle list:
-//   1. counting sort of the block's (cell, id) pairs by cell in shared memory, then insertion sort
-//      by id inside each cell: this is the canonical order (cell key, particle id), written back
-//      to sortedIds;
-//   2. thread c walks the particles of cell c in id order, loading each one a particle ahead,
+//   1. the block's cell ranges come from the per-cell starts of the sort;
+//   2. thread c walks the particles of cell c in sorted order, loading each one a particle ahead,
 //      turns it into the affine contribution u + i*a0 + j*a1 + k*a2 (MLS / PB-MPM) and
 //      accumulates the 27 stencil nodes in registers (the sums inside a block are deterministic);
 //   3. a 27-phase flush adds the registers into a per-warp shared-memory 6x6x6 node tile: in one
 //      phase the 32 lanes of a warp write 32 distinct nodes, so no atomics are needed;
 //   4. the two warp tiles are summed in a fixed order and each touched node gets one float4
 //      vector atomic in the block-major accumulation grid.
-// Particles whose stencil base lies outside the grid, and blocks holding more than kCellCap
-// particles, take a per-particle path with global vector atomics instead.
+// Particles whose stencil base lies outside the grid take a per-particle path with global vector
+// atomics instead, and particles beyond the first kCellRun of a cell are added by vector atomics.
 #pragma once
 
 namespace crb200
 {
-    constexpr int kCellCap = 1024; // particles of one block sorted in shared memory
     constexpr int kRec = 16;       // floats per staged particle
     constexpr int kCellRun = 9;    // particles a cell thread accumulates; the rest of a cell's
                                    // particles go through per-particle vector atomics
@@ -273,98 +270,6 @@ namespace crb200
         }
     }
 
-    // (a) Canonical order inside each active block: counting sort of the block's (cell, id) pairs
-    //     by cell, then insertion sort by id inside each cell.  Writes sortedIds and, per sorted
-    //     slot, the cell (0..63) the slot belongs to.  Blocks above kCellCap particles are ordered
-    //     by rank counting in global memory.
-    __global__ void __launch_bounds__(64) k_cellSort(const SortHeader *__restrict__ hdr, const unsigned *__restrict__ activeList,
-                                                     const unsigned *__restrict__ blockStart,
-                                                     const unsigned long long *__restrict__ pairs,
-                                                     unsigned *__restrict__ sortedIds, unsigned char *__restrict__ sortedCell,
-                                                     unsigned *status)
-    {
-        __shared__ unsigned sIds[kCellCap];
-        __shared__ unsigned sTmp[kCellCap];
-        __shared__ unsigned char sCell[kCellCap];
-        __shared__ unsigned short sRank[kCellCap];
-        __shared__ unsigned sCnt[64];
-        __shared__ unsigned sStart[65];
-        __shared__ unsigned sWarpTot;
-        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        const unsigned nAct = hdr->numActiveBlocks;
-        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
-        {
-            const unsigned b = activeList[ab];
-            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            if (cnt > (unsigned)kCellCap)
-            {
-                if (tid == 0)
-                    atomicOr(status, CRB200_STATUS_BLOCK_OVERFLOW);
-                for (unsigned t = tid; t < cnt; t += 64)
-                {
-                    const unsigned long long e = pairs[start + t];
-                    unsigned rank = 0;
-                    for (unsigned u2 = 0; u2 < cnt; ++u2)
-                        rank += pairs[start + u2] < e;
-                    sortedIds[start + rank] = (unsigned)e;
-                    sortedCell[start + rank] = (unsigned char)(e >> 32);
-                }
-                continue;
-            }
-            sCnt[tid] = 0;
-            __syncthreads();
-            for (unsigned t = tid; t < cnt; t += 64)
-            {
-                const unsigned long long pr = pairs[start + t];
-                const unsigned c = (unsigned)(pr >> 32);
-                sCell[t] = (unsigned char)c;
-                sTmp[t] = (unsigned)pr;
-                sRank[t] = (unsigned short)atomicAdd(&sCnt[c], 1u);
-            }
-            __syncthreads();
-            {
-                const unsigned v = sCnt[tid];
-                unsigned inc = v;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o)
-                        inc += y;
-                }
-                if (tid == 31)
-                    sWarpTot = inc;
-                __syncthreads();
-                const unsigned excl = inc - v + (warp ? sWarpTot : 0u);
-                sStart[tid] = excl;
-                if (tid == 63)
-                    sStart[64] = excl + v;
-            }
-            __syncthreads();
-            for (unsigned t = tid; t < cnt; t += 64)
-                sIds[sStart[sCell[t]] + sRank[t]] = sTmp[t];
-            __syncthreads();
-            const unsigned cs = sStart[tid], ce = sStart[tid + 1];
-            for (unsigned a = cs + 1; a < ce; ++a)
-            {
-                const unsigned key = sIds[a];
-                unsigned j = a;
-                while (j > cs && sIds[j - 1] > key)
-                {
-                    sIds[j] = sIds[j - 1];
-                    --j;
-                }
-                sIds[j] = key;
-            }
-            for (unsigned a = cs; a < ce; ++a)
-                sortedCell[start + a] = (unsigned char)tid;
-            __syncthreads();
-            for (unsigned t = tid; t < cnt; t += 64)
-                sortedIds[start + t] = sIds[t];
-            __syncthreads();
-        }
-    }
-
     // (b) One record per particle (indexed by particle id), particle-parallel over the sorted slots.
     //     Outliers are scattered here with global atomics and leave a zero record.  PB-MPM's
     //     material constraint writes the relaxed C back.  Nothing to do when the previous substep's
@@ -423,12 +328,11 @@ namespace crb200
                                                        const unsigned *__restrict__ activeList,
                                                        const unsigned *__restrict__ blockStart,
                                                        const unsigned *__restrict__ sortedIds,
-                                                       const unsigned char *__restrict__ sortedCell,
+                                                       const unsigned *__restrict__ cellStart,
                                                        const float4 *__restrict__ records,
                                                        const unsigned *__restrict__ cutMasks, float4 *__restrict__ gridA,
                                                        float4 *__restrict__ gridF)
     {
-        __shared__ unsigned sCnt[64];
         __shared__ unsigned sStart[65];
         __shared__ unsigned sOv[65];
         __shared__ unsigned sWarpTot;
@@ -460,29 +364,13 @@ namespace crb200
             const unsigned lb = b - g.blockBase;
             const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
             const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            // cell ranges of this block's sorted slots
-            sCnt[tid] = 0;
-            __syncthreads();
-            for (unsigned t = tid; t < cnt; t += 64)
-                atomicAdd(&sCnt[sortedCell[start + t]], 1u);
-            __syncthreads();
+            // cell ranges of this block's sorted slots (cells are contiguous, in cell order)
             {
-                const unsigned v = sCnt[tid];
-                unsigned inc = v;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o)
-                        inc += y;
-                }
-                if (tid == 31)
-                    sWarpTot = inc;
-                __syncthreads();
-                const unsigned excl = inc - v + (warp ? sWarpTot : 0u);
+                const unsigned excl = cellStart[b * 64u + tid] - start;
+                const unsigned v = (tid < 63 ? cellStart[b * 64u + tid + 1] - start : cnt) - excl;
                 sStart[tid] = excl;
                 if (tid == 63)
-                    sStart[64] = excl + v;
+                    sStart[64] = cnt;
                 // overflow prefix: particles beyond the first kCellRun of each cell
                 const unsigned ov = v > (unsigned)kCellRun ? v - (unsigned)kCellRun : 0u;
                 unsigned oinc = ov;
