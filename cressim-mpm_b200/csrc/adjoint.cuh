@@ -664,7 +664,7 @@ namespace crb200
     void Solver::releaseAdjoint()
     {
         releaseAdjointGraphs();
-        void *bufs[] = {adjCkpt, adjSeg, aX, aV, aMat, aF, aC, gridG, adjForce, adjTorque};
+        void *bufs[] = {adjCkpt, adjSeg, aX, aV, aMat, aF, aC, gridG, adjForce, adjTorque, adjTape};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -672,37 +672,81 @@ namespace crb200
         aX = aV = aMat = nullptr;
         aF = aC = nullptr;
         gridG = adjForce = adjTorque = nullptr;
-        adjCkptCap = adjSegCap = 0;
+        adjCkptCap = adjSegCap = adjTapeCap = 0;
+        adjTape = nullptr;
         adjRecorded = false;
     }
 
     // State blob: x|m (float4 n), v (float4 n), F (9 planes of n), C (9 planes of n).
+    // One kernel moves a particle state between the solver's arrays and a blob (x|m and v as
+    // float4, then F and C as 9 planes of n floats each); loading also clears the bin counters and
+    // the carried-records flag (what invalidateRecords does), so a replayed state costs one graph
+    // node instead of seven.
+    __global__ void k_stateCopy(unsigned n, unsigned stride, bool load, float4 *__restrict__ x, float4 *__restrict__ v,
+                                float *__restrict__ F, float *__restrict__ C, unsigned char *__restrict__ blob,
+                                unsigned *__restrict__ blockCount, unsigned numBlockCounts,
+                                unsigned *__restrict__ cellCount, unsigned numCellCounts, unsigned *__restrict__ flag)
+    {
+        float4 *bx = reinterpret_cast<float4 *>(blob);
+        float4 *bv = bx + n;
+        float *bF = reinterpret_cast<float *>(bv + n);
+        float *bC = bF + 9ull * n;
+        const unsigned stepN = gridDim.x * blockDim.x;
+        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stepN)
+        {
+            if (load)
+            {
+                x[i] = bx[i];
+                v[i] = bv[i];
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                {
+                    F[k * stride + i] = bF[(size_t)k * n + i];
+                    C[k * stride + i] = bC[(size_t)k * n + i];
+                }
+            }
+            else
+            {
+                bx[i] = x[i];
+                bv[i] = v[i];
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                {
+                    bF[(size_t)k * n + i] = F[k * stride + i];
+                    bC[(size_t)k * n + i] = C[k * stride + i];
+                }
+            }
+        }
+        if (load)
+        {
+            for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < numBlockCounts; j += stepN)
+                blockCount[j] = 0u;
+            for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < numCellCounts; j += stepN)
+                cellCount[j] = 0u;
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+                *flag = 0u;
+        }
+    }
+
     int Solver::saveState(unsigned char *dst)
     {
-        const size_t n = totalParticles();
-        const size_t pitch = (size_t)numMaxParticles * sizeof(float);
-        CRB_CHECK(cudaMemcpyAsync(dst, positionMass, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpyAsync(dst + n * 16, velocity, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpy2DAsync(dst + n * 32, n * sizeof(float), F, pitch, n * sizeof(float), 9,
-                                    cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpy2DAsync(dst + n * 68, n * sizeof(float), Cm, pitch, n * sizeof(float), 9,
-                                    cudaMemcpyDeviceToDevice, stream));
+        const unsigned n = totalParticles();
+        if (!n)
+            return CRB200_OK;
+        k_stateCopy<<<std::min((n + 255) / 256, (unsigned)strideCtas), 256, 0, stream>>>(
+            n, (unsigned)numMaxParticles, false, positionMass, velocity, F, Cm, dst, nullptr, 0u, nullptr, 0u, nullptr);
+        CRB_LAUNCHED(1);
         return CRB200_OK;
     }
 
     int Solver::loadState(const unsigned char *src)
     {
-        int rv = invalidateRecords();
-        if (rv != CRB200_OK)
-            return rv;
-        const size_t n = totalParticles();
-        const size_t pitch = (size_t)numMaxParticles * sizeof(float);
-        CRB_CHECK(cudaMemcpyAsync(positionMass, src, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpyAsync(velocity, src + n * 16, n * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpy2DAsync(F, pitch, src + n * 32, n * sizeof(float), n * sizeof(float), 9,
-                                    cudaMemcpyDeviceToDevice, stream));
-        CRB_CHECK(cudaMemcpy2DAsync(Cm, pitch, src + n * 68, n * sizeof(float), n * sizeof(float), 9,
-                                    cudaMemcpyDeviceToDevice, stream));
+        const unsigned n = totalParticles();
+        const unsigned nodes = totalBlocks * 64u;
+        k_stateCopy<<<std::max(1u, std::min((std::max(n, nodes) + 255) / 256, (unsigned)strideCtas)), 256, 0, stream>>>(
+            n, (unsigned)numMaxParticles, true, positionMass, velocity, F, Cm, const_cast<unsigned char *>(src),
+            blockCount, totalBlocks + 1, cellCount, nodes, &header->recordsValid);
+        CRB_LAUNCHED(1);
         return CRB200_OK;
     }
 
@@ -827,12 +871,45 @@ namespace crb200
         return CRB200_OK;
     }
 
-    template <bool Multi>
-    int Solver::adjointSubstep()
+    // Tape layout of one slot (each part 256-byte aligned).
+    size_t Solver::tapeSlotBytes() const
     {
-        int r = launchStepT<Multi>(true); // replay: gridA = (P, M), gridV = V
-        if (r != CRB200_OK)
-            return r;
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t nodes = (size_t)totalBlocks * 64;
+        return 2 * al(nodes * sizeof(float4)) + al((size_t)numMaxParticles * 4) + al(nodes * 4) +
+               3 * al(((size_t)totalBlocks + 1) * 4) + al(sizeof(SortHeader));
+    }
+
+    Solver::TapeSlot Solver::tapeSlot(int k) const
+    {
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t nodes = (size_t)totalBlocks * 64;
+        unsigned char *p = adjTape + (size_t)k * tapeSlotBytes();
+        TapeSlot t;
+        t.gridA = reinterpret_cast<float4 *>(p);
+        p += al(nodes * sizeof(float4));
+        t.gridV = reinterpret_cast<float4 *>(p);
+        p += al(nodes * sizeof(float4));
+        t.sortedIds = reinterpret_cast<unsigned *>(p);
+        p += al((size_t)numMaxParticles * 4);
+        t.cellStart = reinterpret_cast<unsigned *>(p);
+        p += al(nodes * 4);
+        t.blockStart = reinterpret_cast<unsigned *>(p);
+        p += al(((size_t)totalBlocks + 1) * 4);
+        t.activeList = reinterpret_cast<unsigned *>(p);
+        p += al(((size_t)totalBlocks + 1) * 4);
+        t.touchedList = reinterpret_cast<unsigned *>(p);
+        p += al(((size_t)totalBlocks + 1) * 4);
+        t.hdr = reinterpret_cast<SortHeader *>(p);
+        return t;
+    }
+
+    // One reverse substep from the tape of slot k (the replayed forward of the same input state
+    // wrote its P2G grid, grid velocities and sort there); the input state itself is loaded.
+    template <bool Multi>
+    int Solver::adjointSubstepTape(int k)
+    {
+        const TapeSlot ts = tapeSlot(k);
         const StepParams p = params();
         const SceneTable sc = sceneTable();
         const unsigned pg = (sc.numParticles + 127) / 128;
@@ -840,11 +917,11 @@ namespace crb200
                          reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
         const unsigned stride = (unsigned)numMaxParticles;
         CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
-        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, gridV, aX, aV,
-                                                aF, aC, gridG, records);
-        k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, cellStart,
-                                                            records, cutMasks, gridG, gridF);
-        k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridG);
+        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, ts.gridV, aX,
+                                                aV, aF, aC, gridG, records);
+        k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, ts.hdr, ts.activeList, ts.blockStart, ts.sortedIds,
+                                                            ts.cellStart, records, cutMasks, gridG, gridF);
+        k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, ts.hdr, ts.touchedList, shapeTable, sp, ts.gridA, gridG);
         k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, matParams, F, Cm, V0, stride,
                                                 gridG, aX, aV, aF, aC, aMat);
         CRB_LAUNCHED(4);
@@ -875,6 +952,15 @@ namespace crb200
             const int ns = std::max(shapes.size, 1);
             CRB_CHECK(cudaMalloc(&adjForce, ns * sizeof(float4)));
             CRB_CHECK(cudaMalloc(&adjTorque, ns * sizeof(float4)));
+        }
+        if ((size_t)K * tapeSlotBytes() > adjTapeCap)
+        {
+            if (adjTape)
+                cudaFree(adjTape);
+            adjTape = nullptr;
+            adjTapeCap = 0;
+            CRB_CHECK(cudaMalloc(&adjTape, (size_t)K * tapeSlotBytes()));
+            adjTapeCap = (size_t)K * tapeSlotBytes();
         }
         if ((size_t)K * sb > adjSegCap)
         {
@@ -917,19 +1003,7 @@ namespace crb200
         const size_t sb = stateBytes();
         const uint64_t before = launchCount();
         CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        int r;
-        if (which == 0)
-        {
-            r = saveState(adjSeg + (size_t)k * sb);
-            if (r == CRB200_OK)
-                r = launchStep();
-        }
-        else
-        {
-            r = loadState(adjSeg + (size_t)k * sb);
-            if (r == CRB200_OK)
-                r = isBatch() ? adjointSubstep<true>() : adjointSubstep<false>();
-        }
+        const int r = which == 1 ? reverseBody(k, sb) : replayBody(k, sb, which == 2);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(stream, &g);
         const uint64_t captured = launchCount() - before;
@@ -950,29 +1024,55 @@ namespace crb200
         return CRB200_OK;
     }
 
+    // replay slot k: keep the input state, run the forward substep writing slot k's tape (the
+    // segment's last slot: only up to the grid update)
+    int Solver::replayBody(int k, size_t sb, bool last)
+    {
+        int r = saveState(adjSeg + (size_t)k * sb);
+        if (r != CRB200_OK)
+            return r;
+        tapeActive = k;
+        r = last ? (isBatch() ? launchStepT<true>(true) : launchStepT<false>(true)) : launchStep();
+        tapeActive = -1;
+        return r;
+    }
+
+    int Solver::reverseBody(int k, size_t sb)
+    {
+        int r = loadState(adjSeg + (size_t)k * sb);
+        if (r != CRB200_OK)
+            return r;
+        return isBatch() ? adjointSubstepTape<true>(k) : adjointSubstepTape<false>(k);
+    }
+
     void Solver::releaseAdjointGraphs()
     {
-        for (auto &v : {&adjReplayG, &adjReverseG})
+        for (auto &v : {&adjReplayG, &adjReverseG, &adjReplayLastG})
             for (cudaGraphExec_t gx : *v)
                 if (gx)
                     cudaGraphExecDestroy(gx);
         adjReplayG.clear();
         adjReverseG.clear();
-        adjGraphKernels[0] = adjGraphKernels[1] = 0;
+        adjReplayLastG.clear();
+        adjGraphKernels[0] = adjGraphKernels[1] = adjGraphKernels[2] = 0;
     }
 
     int Solver::adjointGraphs(int K)
     {
-        if ((int)adjReplayG.size() == K && adjGraphVersion == configVersion && adjGraphSeg == adjSeg)
+        if ((int)adjReplayG.size() == K && adjGraphVersion == configVersion && adjGraphSeg == adjSeg &&
+            adjGraphTape == adjTape)
             return CRB200_OK;
         releaseAdjointGraphs();
         adjReplayG.assign(K, nullptr);
         adjReverseG.assign(K, nullptr);
+        adjReplayLastG.assign(K, nullptr);
         for (int k = 0; k < K; ++k)
         {
             int r = captureGraph(0, k, &adjReplayG[k], &adjGraphKernels[0]);
             if (r == CRB200_OK)
                 r = captureGraph(1, k, &adjReverseG[k], &adjGraphKernels[1]);
+            if (r == CRB200_OK)
+                r = captureGraph(2, k, &adjReplayLastG[k], &adjGraphKernels[2]);
             if (r != CRB200_OK)
             {
                 releaseAdjointGraphs();
@@ -981,6 +1081,7 @@ namespace crb200
         }
         adjGraphVersion = configVersion;
         adjGraphSeg = adjSeg;
+        adjGraphTape = adjTape;
         return CRB200_OK;
     }
 
@@ -994,21 +1095,19 @@ namespace crb200
         for (int seg = (T - 1) / K; seg >= 0; --seg)
         {
             const int t0 = seg * K, t1 = std::min(T, t0 + K);
-            // replay the segment's inputs s_t0 .. s_(t1-1)
+            // replay the segment's inputs s_t0 .. s_(t1-1), each substep writing its slot's tape
             if ((r = loadState(adjCkpt + (size_t)seg * sb)) != CRB200_OK)
                 return r;
             for (int t = t0; t < t1; ++t)
             {
                 const int k = t - t0;
-                if (t + 1 < t1 && graphs)
+                const bool last = t + 1 == t1;
+                if (graphs)
                 {
-                    CRB_CHECK(cudaGraphLaunch(adjReplayG[k], stream));
-                    noteLaunches(adjGraphKernels[0]);
-                    continue;
+                    CRB_CHECK(cudaGraphLaunch(last ? adjReplayLastG[k] : adjReplayG[k], stream));
+                    noteLaunches(adjGraphKernels[last ? 2 : 0]);
                 }
-                if ((r = saveState(adjSeg + (size_t)k * sb)) != CRB200_OK)
-                    return r;
-                if (t + 1 < t1 && (r = launchStep()) != CRB200_OK)
+                else if ((r = replayBody(k, sb, last)) != CRB200_OK)
                     return r;
             }
             for (int t = t1; t > t0; --t)
@@ -1024,12 +1123,8 @@ namespace crb200
                 {
                     CRB_CHECK(cudaGraphLaunch(adjReverseG[k], stream));
                     noteLaunches(adjGraphKernels[1]);
-                    continue;
                 }
-                if ((r = loadState(adjSeg + (size_t)k * sb)) != CRB200_OK)
-                    return r;
-                r = isBatch() ? adjointSubstep<true>() : adjointSubstep<false>();
-                if (r != CRB200_OK)
+                else if ((r = reverseBody(k, sb)) != CRB200_OK)
                     return r;
             }
         }

@@ -174,17 +174,32 @@ namespace crb200
         int captureGraph(int which, int k, cudaGraphExec_t *out, int *kernels);
         int adjointGraphs(int K);
         void releaseAdjointGraphs();
-        std::vector<cudaGraphExec_t> adjReplayG, adjReverseG;
-        int adjGraphKernels[2] = {0, 0};
+        std::vector<cudaGraphExec_t> adjReplayG, adjReverseG, adjReplayLastG;
+        // the adjoint's per-slot tape of a replayed substep: its P2G grid, grid velocities and sort
+        struct TapeSlot
+        {
+            float4 *gridA, *gridV;
+            unsigned *sortedIds, *cellStart, *blockStart, *activeList, *touchedList;
+            SortHeader *hdr;
+        };
+        unsigned char *adjTape = nullptr;
+        size_t adjTapeCap = 0;
+        int tapeActive = -1; // slot the running forward substep writes its tape to (-1: none)
+        size_t tapeSlotBytes() const;
+        TapeSlot tapeSlot(int k) const;
+        template <bool Multi>
+        int adjointSubstepTape(int k);
+        int adjGraphKernels[3] = {0, 0, 0};
         unsigned adjGraphVersion = ~0u;
-        unsigned char *adjGraphSeg = nullptr;
+        unsigned char *adjGraphSeg = nullptr, *adjGraphTape = nullptr;
+        int replayBody(int k, size_t sb, bool last);
+        int reverseBody(int k, size_t sb);
         void releaseAdjoint();
         int adjointCheck();
         int saveState(unsigned char *dst);
         int invalidateRecords();
         int loadState(const unsigned char *src);
-        template <bool Multi>
-        int adjointSubstep();
+
         size_t stateBytes() const { return (size_t)totalParticles() * (2 * sizeof(float4) + 18 * sizeof(float)); }
         int adjSubsteps = 0, adjInterval = 0;
         std::vector<int> adjCaptures;

@@ -534,7 +534,8 @@ namespace crb200
                                                         float4 *__restrict__ gridA, float4 *__restrict__ gridF,
                                                         float4 *__restrict__ gridV, float4 *coupleForce,
                                                         float4 *coupleTorque, bool clearA,
-                                                        unsigned long long *__restrict__ blockShapeMask)
+                                                        unsigned long long *__restrict__ blockShapeMask,
+                                                        float4 *__restrict__ saveA, float4 *__restrict__ saveV)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
@@ -579,6 +580,8 @@ namespace crb200
             float4 acc = gridA[a];
             if (clearA)
                 gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (saveA)
+                saveA[a] = acc; // the adjoint's tape of this substep's P2G grid
             float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
             if (withForce)
             {
@@ -595,6 +598,8 @@ namespace crb200
             if (acc.w < p.cutoff)
             {
                 gridV[a] = acc; // light nodes keep momentum, which G2P then reads (reference Q2)
+                if (saveV)
+                    saveV[a] = acc;
                 continue;
             }
             if (withForce)
@@ -616,6 +621,8 @@ namespace crb200
             if (k < 2 || k > g.n.z - 3)
                 v.z = 0.f;
             gridV[a] = make_float4(v.x, v.y, v.z, acc.w);
+            if (saveV)
+                saveV[a] = make_float4(v.x, v.y, v.z, acc.w);
         }
         __syncthreads();
         if (threadIdx.x == 0 && sTouched)
@@ -1134,6 +1141,33 @@ namespace crb200
         }
     }
 
+    // The adjoint's tape of one substep's sort products (read back by its reverse substep).
+    __global__ void k_tapeSort(unsigned n, unsigned blocks, const unsigned *__restrict__ sortedIds,
+                               const unsigned *__restrict__ cellStart, const unsigned *__restrict__ blockStart,
+                               const unsigned *__restrict__ activeList, const unsigned *__restrict__ touchedList,
+                               const SortHeader *__restrict__ hdr, unsigned *__restrict__ tIds, unsigned *__restrict__ tCell,
+                               unsigned *__restrict__ tStart, unsigned *__restrict__ tActive,
+                               unsigned *__restrict__ tTouched, SortHeader *__restrict__ tHdr)
+    {
+        const unsigned stepN = gridDim.x * blockDim.x, i0 = blockIdx.x * blockDim.x + threadIdx.x;
+        const unsigned nSorted = min(hdr->numSorted, n), nAct = hdr->numActiveBlocks, nT = hdr->numTouchedBlocks;
+        for (unsigned i = i0; i < nSorted; i += stepN)
+            tIds[i] = sortedIds[i];
+        for (unsigned i = i0; i < nAct * 64u; i += stepN)
+        {
+            const unsigned c = activeList[i >> 6] * 64u + (i & 63u);
+            tCell[c] = cellStart[c];
+        }
+        for (unsigned i = i0; i <= blocks; i += stepN)
+            tStart[i] = blockStart[i];
+        for (unsigned i = i0; i < nAct; i += stepN)
+            tActive[i] = activeList[i];
+        for (unsigned i = i0; i < nT; i += stepN)
+            tTouched[i] = touchedList[i];
+        if (i0 == 0)
+            *tHdr = *hdr;
+    }
+
     // Cell keys of the most recent sort, rebuilt from its products (the per-particle key array
     // may already hold the next substep's keys, which G2P writes).
     __global__ void __launch_bounds__(64) k_sortKeysOut(const SortHeader *__restrict__ hdr,
@@ -1493,8 +1527,10 @@ namespace crb200
         return launchStepT<false>(false);
     }
 
-    // recompute: the adjoint's forward replay of one MLS substep up to the grid update, which
-    // keeps the P2G grid (momentum, mass) in gridA and sends coupling forces to scratch.
+    // recompute: a forward substep up to the grid update only (the adjoint's replay of a segment's
+    // last input state); coupling forces go to scratch.  With a tape slot active (tapeActive) the
+    // grid update also writes the P2G grid and the grid velocities to that slot, and the sort
+    // products are copied there; otherwise recompute keeps the P2G grid in gridA.
     template <bool Multi>
     int Solver::launchStepT(bool recompute)
     {
@@ -1570,9 +1606,19 @@ namespace crb200
         auto update = [&]() -> int {
             k_gridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV,
                                                              (recompute || adjReplay) ? adjForce : cf,
-                                                             (recompute || adjReplay) ? adjTorque : ct, !recompute,
-                                                             blockShapeMask);
+                                                             (recompute || adjReplay) ? adjTorque : ct,
+                                                             !recompute || tapeActive >= 0,
+                                                             blockShapeMask, tapeActive >= 0 ? tapeSlot(tapeActive).gridA : nullptr,
+                                                             tapeActive >= 0 ? tapeSlot(tapeActive).gridV : nullptr);
             CRB_LAUNCHED(1);
+            if (tapeActive >= 0)
+            {
+                const TapeSlot ts = tapeSlot(tapeActive);
+                k_tapeSort<<<strideCtas, 256, 0, stream>>>(totalParticles(), totalBlocks, sortedIds, cellStart, blockStart,
+                                                          activeList, touchedList, header, ts.sortedIds, ts.cellStart,
+                                                          ts.blockStart, ts.activeList, ts.touchedList, ts.hdr);
+                CRB_LAUNCHED(1);
+            }
             return CRB200_OK;
         };
         auto g2p = [&](auto mode) -> int {
