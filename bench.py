@@ -206,7 +206,7 @@ def run_ours(args, rank, world, local):
     stream = ds.stream
     # warm-up (graph capture happens on the first replay), then the launch-shape autotuner
     ds.step(max(args.warmup, 3))
-    tuned = s.autotune(10)
+    tuned = (0, 0, 0) if args.quick else s.autotune(10)  # --quick: short runs for profiler launch lists
     ds.step(3)
     ds.sync()
     st = s.grid_stats()
