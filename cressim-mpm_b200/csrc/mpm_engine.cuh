@@ -154,6 +154,7 @@ namespace crb200
         int sortCtas = 0;
         int updCtas = 0;
         int strideCtas = 0;
+        int cellCtas = 0;
 
         cudaGraphExec_t graph = nullptr;
         unsigned graphVersion = ~0u;

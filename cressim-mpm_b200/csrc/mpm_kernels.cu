@@ -487,36 +487,39 @@ namespace crb200
             sortedIds[slot] = i;
     }
 
-    // Absolute start of every cell of the active blocks (one 64-thread CTA per block, one thread per
-    // cell): the block's start plus the exclusive prefix of its cell counts, which are cleared for
-    // the next binning.
-    __global__ void __launch_bounds__(64) k_cellStarts(const SortHeader *__restrict__ hdr,
-                                                       const unsigned *__restrict__ activeList,
-                                                       const unsigned *__restrict__ blockStart,
-                                                       unsigned *__restrict__ cellCount, unsigned *__restrict__ cellStart)
+    // Absolute start of every cell of the active blocks (one warp per block, lane l scanning cells l
+    // and l + 32): the block's start plus the exclusive prefix of its cell counts, which are cleared
+    // for the next binning.
+    __global__ void __launch_bounds__(256) k_cellStarts(const SortHeader *__restrict__ hdr,
+                                                        const unsigned *__restrict__ activeList,
+                                                        const unsigned *__restrict__ blockStart,
+                                                        unsigned *__restrict__ cellCount, unsigned *__restrict__ cellStart)
     {
-        __shared__ unsigned warpTot;
-        const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const unsigned lane = threadIdx.x & 31;
+        const unsigned nWarps = (gridDim.x * blockDim.x) >> 5;
         const unsigned nAct = hdr->numActiveBlocks;
-        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        for (unsigned ab = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ab < nAct; ab += nWarps)
         {
             const unsigned b = activeList[ab];
-            const unsigned c = b * 64u + tid;
-            const unsigned v = cellCount[c];
-            cellCount[c] = 0u;
-            unsigned inc = v;
+            const unsigned c0 = b * 64u + lane, c1 = c0 + 32u;
+            const unsigned v0 = cellCount[c0], v1 = cellCount[c1];
+            cellCount[c0] = 0u;
+            cellCount[c1] = 0u;
+            unsigned i0 = v0, i1 = v1;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1)
             {
-                const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+                const unsigned y0 = __shfl_up_sync(0xffffffffu, i0, o), y1 = __shfl_up_sync(0xffffffffu, i1, o);
                 if (lane >= (unsigned)o)
-                    inc += y;
+                {
+                    i0 += y0;
+                    i1 += y1;
+                }
             }
-            if (tid == 31)
-                warpTot = inc;
-            __syncthreads();
-            cellStart[c] = blockStart[b] + inc - v + (warp ? warpTot : 0u);
-            __syncthreads();
+            const unsigned firstHalf = __shfl_sync(0xffffffffu, i0, 31);
+            const unsigned bs = blockStart[b];
+            cellStart[c0] = bs + i0 - v0;
+            cellStart[c1] = bs + firstHalf + i1 - v1;
         }
     }
 
@@ -1468,8 +1471,8 @@ namespace crb200
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0, false>, 64, 0));
         p2gCtas = sms * (perSm > 0 ? perSm : 1);
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cellStarts, 64, 0));
-        sortCtas = sms * (perSm > 0 ? perSm : 1);
+        sortCtas = sms * 4;  // 64-thread CTAs of the on-request sort-state kernel
+        cellCtas = sms * 4;  // 256-thread CTAs of k_cellStarts (one warp per active block)
         updCtas = sms * 8;
         CRB_CHECK(cudaStreamCreateWithFlags(&sideStream, cudaStreamNonBlocking));
         CRB_CHECK(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming));
@@ -1510,7 +1513,7 @@ namespace crb200
         CRB_LAUNCHED(3);
         if (n > 0)
         {
-            k_cellStarts<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, cellCount, cellStart);
+            k_cellStarts<<<cellCtas, 256, 0, stream>>>(header, activeList, blockStart, cellCount, cellStart);
             k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, cellStart, sortedIds, (unsigned)numMaxParticles);
             CRB_LAUNCHED(1);
         }
@@ -1851,7 +1854,7 @@ namespace crb200
         int dev = 0, sms = 0;
         CRB_CHECK(cudaGetDevice(&dev));
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const int baseP2g = p2gBase > 0 ? p2gBase : p2gCtas, baseSort = sortBase > 0 ? sortBase : sortCtas;
+        const int baseP2g = p2gBase > 0 ? p2gBase : p2gCtas, baseSort = sortBase > 0 ? sortBase : cellCtas;
         p2gBase = baseP2g;
         sortBase = baseSort;
         unsigned char *snap = nullptr;
@@ -1879,7 +1882,7 @@ namespace crb200
                 {
                     updCtas = sms * upd[a];
                     p2gCtas = baseP2g * mul[b];
-                    sortCtas = baseSort * mul[c];
+                    cellCtas = baseSort * mul[c];
                     configVersion++;
                     if ((r = loadState(snap)) != CRB200_OK || (r = stepMany(2)) != CRB200_OK)
                         break; // builds the graph
@@ -1907,7 +1910,7 @@ namespace crb200
         adjReplay = replay0;
         updCtas = sms * bestC[0];
         p2gCtas = baseP2g * bestC[1];
-        sortCtas = baseSort * bestC[2];
+        cellCtas = baseSort * bestC[2];
         configVersion++;
         if (r == CRB200_OK)
             r = loadState(snap);

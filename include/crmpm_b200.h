@@ -267,8 +267,8 @@ CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[
                                          int *outSubsteps, int reset);
 
 /* Launch-shape autotuner (no counterpart in the reference): times the candidate CTA counts of
- * the grid update (4, 8 or 16 per SM), the cell accumulation and the per-block cell sort (1x or 2x
- * their occupancy) over substepsPerTrial substeps each (0: 8) from the current state, keeps the
+ * the grid update (4, 8 or 16 per SM), the cell accumulation (1x or 2x its occupancy) and the
+ * per-cell start computation (4 or 8 per SM) over substepsPerTrial substeps each (0: 8) from the current state, keeps the
  * fastest and restores the state; coupling forces of the trials are not reported.  Writes the
  * choice (update CTAs per SM, accumulation multiple, sort multiple) to outChoiceHost[3] if
  * given.  Needs a non-default solver stream; synchronizes it. */
