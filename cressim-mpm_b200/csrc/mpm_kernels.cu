@@ -254,10 +254,12 @@ namespace crb200
         const unsigned n = Multi ? sc.numParticles : p.numActive;
         unsigned key = kInvalidKey;
         bool ood = false;
+        bool carried = false; // batch: binned by the previous G2P (scene without a slicer)
         if (i < n && (ignoreMask || mask[i]))
         {
             const unsigned short si = Multi ? sc.particleScene[i] : 0;
-            if (!Multi || si != 0xFFFF)
+            carried = Multi && si != 0xFFFF && hdr->recordsValid && !(sc.flags[si] & SF_SLICER);
+            if ((!Multi || si != 0xFFFF) && !carried)
             {
                 const GridGeom &g = Multi ? sc.params[si].g : p.g;
                 const float4 x = xm[i];
@@ -268,7 +270,8 @@ namespace crb200
                     ood = true;
             }
         }
-        binAggregated(0xffffffffu, lane, key, blockCount, cellCount, i < n ? &keys[i] : nullptr, i < n ? &ranks[i] : nullptr);
+        const bool write = i < n && !carried;
+        binAggregated(0xffffffffu, lane, key, blockCount, cellCount, write ? &keys[i] : nullptr, write ? &ranks[i] : nullptr);
         if (__any_sync(0xffffffffu, ood) && lane == 0)
             atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
     }
@@ -742,8 +745,11 @@ namespace crb200
                                                  unsigned *__restrict__ cellCount,
                                                  const unsigned long long *__restrict__ blockShapeMask)
     {
-        constexpr bool kRecords = Mode == 0 && !Multi;
-        const bool writeRecords = kRecords && records != nullptr && !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER));
+        // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
+        // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
+        constexpr bool kRecords = Mode == 0;
+        const bool writeRecords =
+            kRecords && records != nullptr && (Multi || !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER)));
         if (writeRecords && blockIdx.x == 0 && threadIdx.x == 0)
             hdr->recordsValid = 1u; // read only by later launches
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
@@ -914,7 +920,7 @@ namespace crb200
             storeM3(Cm, stride, i, Cn);
         if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)))
             atomicOr(status, CRB200_STATUS_NAN_STATE);
-        if (kRecords && writeRecords)
+        if (kRecords && writeRecords && !(Multi && (sc.flags[si] & SF_SLICER)))
         {
             RawParticle raw;
             raw.x4 = make_float4(xn.x, xn.y, xn.z, x4.w);
@@ -1630,7 +1636,7 @@ namespace crb200
                 return CRB200_OK;
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
-                                                    (M == 0 && !Multi) ? records : nullptr, gridA, header, keys, ranks,
+                                                    M == 0 ? records : nullptr, gridA, header, keys, ranks,
                                                     blockCount, cellCount, blockShapeMask);
             CRB_LAUNCHED(1);
             return CRB200_OK;

@@ -284,13 +284,16 @@ namespace crb200
                                                     const unsigned *__restrict__ cutMasks, float4 *__restrict__ records,
                                                     float4 *__restrict__ gridA, float4 *__restrict__ gridF, unsigned *fp64Count)
     {
-        if (hdr->recordsValid)
+        if (!Multi && hdr->recordsValid)
             return;
+        const bool carry = Multi && hdr->recordsValid;
         const unsigned nS = hdr->numSorted;
         for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < nS; j += gridDim.x * blockDim.x)
         {
         const unsigned id = sortedIds[j];
         const unsigned si = Multi ? sc.particleScene[id] : 0u; // sorted particles have a scene
+        if (carry && !(sc.flags[si] & SF_SLICER))
+            continue; // the previous G2P wrote this particle's record
         const StepParams &p = Multi ? sc.params[si] : p0;
         const bool slicers = Mode <= 1 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
         const unsigned msk = slicers ? cutMasks[id] : 0u;

@@ -64,8 +64,11 @@ def test_mls_batch_matches_oracle():
 
 
 def test_mixed_contact_batch_matches_scenes_alone():
-    """Different grids, shape kinds and SDF-backed geometry in one batch (shape ids are global)."""
-    kinds = ["box", "sphere", "capsule", "trimesh", "lines", "arc", "dynamic_sphere", "effmass_sphere"]
+    """Different grids, shape kinds and SDF-backed geometry in one batch (shape ids are global).
+    The slicer scenes next to slicer-free ones exercise the per-particle choice between records
+    carried from the previous G2P and records built from the stored state."""
+    kinds = ["box", "sphere", "capsule", "trimesh", "lines", "arc", "dynamic_sphere", "effmass_sphere",
+             "quad_slicer", "mesh_slicer"]
     sl = [scenes.contact_scene(k) for k in kinds]
     # the coupling scenes exchange forces through global shape ids: compare them too
     b = _check_against_alone(sl, 30, graph=False)
