@@ -851,15 +851,17 @@ namespace crb200
 
     // Rotation the reference's PB-MPM constraint blends toward: `u * vt` of svd3(targetF), which
     // factors targetF^T (svd3.h:1271-1274) and therefore equals R^T = V U^T for targetF = U S V^T.
-    // Float first; a near-degenerate spectrum (tiny or nearly equal singular values) is redone
-    // in double precision.
+    // V U^T is the polar factor (A (A^T A)^(-1/2))^T: it does not depend on how U and V are chosen
+    // inside a near-degenerate singular subspace, so nearly equal positive singular values need no
+    // care.  Float first; the ill-conditioned cases are redone in double precision: a tiny smallest
+    // singular value, or an inverted matrix (negative smallest singular value) whose two smallest
+    // magnitudes nearly tie (the closest rotation is then ambiguous).
     __device__ __forceinline__ M3 pbRotationTarget(const M3 &A, unsigned *fp64Count)
     {
         float U[9], V[9], s[3];
         svdRotations<float>(A.m, U, V, s, 5);
         const float smax = fabsf(s[0]);
-        const bool degenerate = !(fabsf(s[2]) > 1e-3f * smax) || (s[0] - s[1] < 1e-4f * smax) ||
-                                (s[1] - fabsf(s[2]) < 1e-4f * smax);
+        const bool degenerate = !(fabsf(s[2]) > 1e-3f * smax) || (s[2] < 0.f && s[1] - fabsf(s[2]) < 1e-4f * smax);
         M3 R;
         if (degenerate)
         {
@@ -874,7 +876,12 @@ namespace crb200
                 for (int r = 0; r < 3; ++r)
                     R.m[c * 3 + r] = (float)(Vd[r] * Ud[c] + Vd[3 + r] * Ud[3 + c] + Vd[6 + r] * Ud[6 + c]);
             if (fp64Count)
-                atomicAdd(fp64Count, 1u);
+            {
+                // one atomic per warp: the lanes taking this branch
+                const unsigned am = __activemask();
+                if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1))
+                    atomicAdd(fp64Count, (unsigned)__popc(am));
+            }
         }
         else
         {
