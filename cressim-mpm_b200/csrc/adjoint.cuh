@@ -724,7 +724,10 @@ namespace crb200
             for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < numCellCounts; j += stepN)
                 cellCount[j] = 0u;
             if (blockIdx.x == 0 && threadIdx.x == 0)
-                *flag = 0u;
+            {
+                flag[0] = 0u; // recordsValid
+                flag[1] = 0u; // pbRecordsValid
+            }
         }
     }
 

@@ -65,7 +65,8 @@ namespace crb200
         unsigned fp64Fallbacks;
         unsigned shapeFlags;
         unsigned touchedNodes;
-        unsigned recordsValid; // set by G2P when it binned the particles and wrote the next P2G records
+        unsigned recordsValid;   // set by G2P when it binned the particles and wrote the next P2G records
+        unsigned pbRecordsValid; // PB-MPM: set by the G2P of an iteration that wrote the next iteration's records
     };
 
     class Solver

@@ -732,7 +732,7 @@ namespace crb200
     //    and mark the records valid; particles whose new stencil leaves the grid are scattered into
     //    the (cleared) accumulation grid here, as k_record does.
     template <int Mode, bool Multi>
-    __global__ void __launch_bounds__(128, (Mode == 0 && !Multi) ? 7 : 6) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
+    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : ((Mode == 0 && !Multi) ? 7 : 6)) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
                                                  float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
                                                  float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -747,6 +747,8 @@ namespace crb200
     {
         // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
         // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
+        if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)
+            hdr->pbRecordsValid = records != nullptr ? 1u : 0u; // read only by later launches
         constexpr bool kRecords = Mode == 0;
         const bool writeRecords =
             kRecords && records != nullptr && (Multi || !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER)));
@@ -893,6 +895,37 @@ namespace crb200
         {
             vel[i] = make_float4(va.x, va.y, va.z, 0.f);
             storeM3(Cm, stride, i, Cn);
+            if (records)
+            {
+                // the next iteration's P2G record: the material constraint on the new C (which
+                // stores the relaxed C) and the record, as k_record would build them
+                RawParticle raw;
+                raw.x4 = x4;
+                raw.v4 = make_float4(va.x, va.y, va.z, 0.f);
+                raw.mp = matParams[i];
+                raw.mt = matType[i];
+                M3 Fp;
+                loadM3(F, stride, i, Fp);
+#pragma unroll
+                for (int e = 0; e < 9; ++e)
+                {
+                    raw.F[e] = Fp.m[e];
+                    raw.C[e] = Cn.m[e];
+                }
+                raw.v0 = 0.f;
+                float rec[kRec];
+                if (!buildRecord<1>(p, i, raw, Cm, stride, msk, true, gridA, nullptr, &hdr->fp64Fallbacks, rec))
+                {
+#pragma unroll
+                    for (int e = 0; e < kRec; ++e)
+                        rec[e] = 0.f;
+                }
+                float4 *out = records + 4ull * i;
+                out[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+                out[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+                out[2] = make_float4(rec[8], rec[9], rec[10], rec[11]);
+                out[3] = make_float4(rec[12], rec[13], rec[14], rec[15]);
+            }
             return;
         }
         V3 xn = x + va * p.dt;
@@ -1630,13 +1663,14 @@ namespace crb200
             }
             return CRB200_OK;
         };
-        auto g2p = [&](auto mode) -> int {
+        // pbRecords: PB-MPM iterations but the last build the next iteration's records in G2P
+        auto g2p = [&](auto mode, bool pbRecords = false) -> int {
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
-                                                    M == 0 ? records : nullptr, gridA, header, keys, ranks,
+                                                    (M == 0 || (M == 1 && pbRecords)) ? records : nullptr, gridA, header, keys, ranks,
                                                     blockCount, cellCount, blockShapeMask);
             CRB_LAUNCHED(1);
             return CRB200_OK;
@@ -1662,7 +1696,7 @@ namespace crb200
                 if (it == 0) markPhase(2);
                 if ((r = update()) != CRB200_OK) return r;
                 if (it == 0) markPhase(3);
-                if ((r = g2p(M1{})) != CRB200_OK) return r;
+                if ((r = g2p(M1{}, it + 1 < iterations)) != CRB200_OK) return r;
             }
             if (pg)
             {
@@ -1757,7 +1791,7 @@ namespace crb200
     // flag, so that k_bin starts from zero counts.
     int Solver::invalidateRecords()
     {
-        CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, sizeof(unsigned), stream));
+        CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, 2 * sizeof(unsigned), stream)); // + pbRecordsValid
         CRB_CHECK(cudaMemsetAsync(blockCount, 0, (totalBlocks + 1) * sizeof(unsigned), stream));
         CRB_CHECK(cudaMemsetAsync(cellCount, 0, (size_t)totalBlocks * 64 * sizeof(unsigned), stream));
         return CRB200_OK;

@@ -273,7 +273,7 @@ namespace crb200
     // (b) One record per particle (indexed by particle id), particle-parallel over the sorted slots.
     //     Outliers are scattered here with global atomics and leave a zero record.  PB-MPM's
     //     material constraint writes the relaxed C back.  Nothing to do when the previous substep's
-    //     G2P already wrote the records (hdr->recordsValid).
+    //     G2P already wrote the records (hdr->recordsValid; PB-MPM: hdr->pbRecordsValid).
     template <int Mode, bool Multi>
     __global__ void __launch_bounds__(128, Mode == 1 ? 4 : 8) k_record(const __grid_constant__ StepParams p0, SceneTable sc,
                                                     const SortHeader *__restrict__ hdr,
@@ -284,9 +284,9 @@ namespace crb200
                                                     const unsigned *__restrict__ cutMasks, float4 *__restrict__ records,
                                                     float4 *__restrict__ gridA, float4 *__restrict__ gridF, unsigned *fp64Count)
     {
-        if (!Multi && hdr->recordsValid)
+        if ((Mode == 0 && !Multi && hdr->recordsValid) || (Mode == 1 && hdr->pbRecordsValid))
             return;
-        const bool carry = Multi && hdr->recordsValid;
+        const bool carry = Mode == 0 && Multi && hdr->recordsValid;
         const unsigned nS = hdr->numSorted;
         for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < nS; j += gridDim.x * blockDim.x)
         {
