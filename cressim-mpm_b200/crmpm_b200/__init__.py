@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
         "CrB200SolverClearStatus": (i, [vp]),
         "CrB200SolverSetOption": (i, [vp, i, i]),
         "CrB200SolverAdvance": (i, [vp, f, vp, vp, C.POINTER(i)]),
+        "CrB200SolverAdvanceAsync": (i, [vp, f, vp, vp, C.POINTER(i)]),
         "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
         "CrB200SolverGetGridStats": (i, [vp, vp]),
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
@@ -298,6 +299,13 @@ class GpuSolver:
         n = C.c_int()
         check(lib().CrB200SolverAdvance(self._h, C.c_float(dt), C.c_void_p(host_pos_ptr), C.c_void_p(host_vel_ptr),
                                         C.byref(n)), "advance")
+        return n.value
+
+    def advance_async(self, dt: float, host_pos_ptr: int = 0, host_vel_ptr: int = 0) -> int:
+        """advance without waiting: the readback into the host buffers completes by fetch_results()."""
+        n = C.c_int()
+        check(lib().CrB200SolverAdvanceAsync(self._h, C.c_float(dt), C.c_void_p(host_pos_ptr),
+                                             C.c_void_p(host_vel_ptr), C.byref(n)), "advance_async")
         return n.value
 
     def phase_times(self, reset: bool = True):

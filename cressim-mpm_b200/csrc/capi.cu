@@ -559,6 +559,23 @@ extern "C"
                           outSubsteps);
     }
 
+    CRB200_API int CrB200SolverAdvanceAsync(CrB200SolverHandle solver, float dt, CrB200Float4 *positionMassHost,
+                                            CrB200Float4 *velocityHost, int *outSubsteps)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (!s->initialized)
+        {
+            crb200::setLastError("CrB200SolverAdvanceAsync: solver not initialized");
+            return CRB200_ERR_NOT_INITIALIZED;
+        }
+        if (!(dt >= 0.f))
+            return bad("CrB200SolverAdvanceAsync: dt must be non-negative");
+        if (!(dt <= s->dt * 1.0e6f))
+            return bad("CrB200SolverAdvanceAsync: dt spans more than a million substeps");
+        return s->advanceAsync(dt, reinterpret_cast<float4 *>(positionMassHost),
+                               reinterpret_cast<float4 *>(velocityHost), outSubsteps);
+    }
+
     CRB200_API int CrB200SolverAutotune(CrB200SolverHandle solver, int substepsPerTrial, int *outChoiceHost)
     {
         SOLVER_OR_FAIL(solver);

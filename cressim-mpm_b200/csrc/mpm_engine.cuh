@@ -88,6 +88,10 @@ namespace crb200
         int autotune(int trial, int choice[3]);
         int p2gBase = 0, sortBase = 0; // occupancy-derived CTA counts the autotuner multiplies
         int advance(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
+        int advanceAsync(float dt, float4 *hostX, float4 *hostV, int *outSubsteps);
+        cudaStream_t copyStream = nullptr; // host readback of advanceAsync
+        cudaEvent_t stagedEvent = nullptr, copiedEvent = nullptr;
+        float4 *stageX = nullptr, *stageV = nullptr;
         int collectPhaseTimes();
 
         // configuration (MpmSolver setters / binders)

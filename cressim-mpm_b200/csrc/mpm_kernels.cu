@@ -1422,8 +1422,17 @@ namespace crb200
             if (b)
                 cudaFree(b);
         releaseAdjoint();
-        if (forkEvent)
-            cudaEventDestroy(forkEvent);
+        if (copiedEvent)
+            cudaEventSynchronize(copiedEvent);
+        for (cudaEvent_t e : {forkEvent, stagedEvent, copiedEvent})
+            if (e)
+                cudaEventDestroy(e);
+        if (copyStream)
+            cudaStreamDestroy(copyStream);
+        if (stageX)
+            cudaFree(stageX);
+        if (stageV)
+            cudaFree(stageV);
         if (joinEvent)
             cudaEventDestroy(joinEvent);
         if (sideStream)
@@ -1774,6 +1783,63 @@ namespace crb200
         return CRB200_OK;
     }
 
+    // Asynchronous variant of advance: the substeps, a device-side snapshot of x and v, and their
+    // copy to the host on a separate copy stream are enqueued, and the call returns; the next
+    // frame's substeps overlap this frame's readback.  fetchResults waits for both.
+    int Solver::advanceAsync(float dtFrame, float4 *hostX, float4 *hostV, int *outSubsteps)
+    {
+        for (const auto &d : batch)
+            if (d.dt != dt)
+            {
+                setLastError("advance: the scenes of this batch have different substep sizes");
+                return CRB200_ERR_UNSUPPORTED;
+            }
+        if (stream == nullptr)
+        {
+            setLastError("advanceAsync: needs a non-default solver stream");
+            return CRB200_ERR_UNSUPPORTED;
+        }
+        float t = 0.f;
+        int n = 0;
+        while (t < dtFrame)
+        {
+            t += dt;
+            ++n;
+        }
+        int r = stepMany(n);
+        if (r != CRB200_OK)
+            return r;
+        const unsigned nPart = totalParticles();
+        if ((hostX || hostV) && nPart)
+        {
+            if (!copyStream)
+            {
+                CRB_CHECK(cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking));
+                CRB_CHECK(cudaEventCreateWithFlags(&stagedEvent, cudaEventDisableTiming));
+                CRB_CHECK(cudaEventCreateWithFlags(&copiedEvent, cudaEventDisableTiming));
+                CRB_CHECK(cudaMalloc(&stageX, (size_t)numMaxParticles * sizeof(float4)));
+                CRB_CHECK(cudaMalloc(&stageV, (size_t)numMaxParticles * sizeof(float4)));
+                CRB_CHECK(cudaEventRecord(copiedEvent, copyStream));
+            }
+            // the previous frame's host copy must be done with the staging buffers
+            CRB_CHECK(cudaStreamWaitEvent(stream, copiedEvent, 0));
+            if (hostX)
+                CRB_CHECK(cudaMemcpyAsync(stageX, positionMass, nPart * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+            if (hostV)
+                CRB_CHECK(cudaMemcpyAsync(stageV, velocity, nPart * sizeof(float4), cudaMemcpyDeviceToDevice, stream));
+            CRB_CHECK(cudaEventRecord(stagedEvent, stream));
+            CRB_CHECK(cudaStreamWaitEvent(copyStream, stagedEvent, 0));
+            if (hostX)
+                CRB_CHECK(cudaMemcpyAsync(hostX, stageX, nPart * sizeof(float4), cudaMemcpyDeviceToHost, copyStream));
+            if (hostV)
+                CRB_CHECK(cudaMemcpyAsync(hostV, stageV, nPart * sizeof(float4), cudaMemcpyDeviceToHost, copyStream));
+            CRB_CHECK(cudaEventRecord(copiedEvent, copyStream));
+        }
+        if (outSubsteps)
+            *outSubsteps = n;
+        return CRB200_OK;
+    }
+
     int Solver::step()
     {
         if (!initialized)
@@ -1985,6 +2051,8 @@ namespace crb200
 
     int Solver::fetchResults()
     {
+        if (copiedEvent)
+            CRB_CHECK(cudaEventSynchronize(copiedEvent));
         CRB_CHECK(cudaStreamSynchronize(stream));
         return CRB200_OK;
     }

@@ -186,6 +186,17 @@ CRB200_API int CrB200SolverComputeInitialData(CrB200SolverHandle solver, unsigne
 CRB200_API int CrB200SolverAdvance(CrB200SolverHandle solver, float dt, CrB200Float4 *positionMassHost,
                                    CrB200Float4 *velocityHost, int *outSubsteps);
 
+/* Asynchronous CrB200SolverAdvance, as the reference's Scene::advance / fetchResults pair works
+ * (scene_impl.cpp:290-330: advance starts the task, fetchResults waits): the substeps, a device
+ * snapshot of positionMass and velocity and its copy into the host buffers (on a separate copy
+ * stream) are enqueued and the call returns, so that the next call's substeps run while this
+ * call's copy is in flight.  The host buffers must not be read or freed before
+ * CrB200SolverFetchResults returns, which waits for the substeps and all copies; copies into one
+ * buffer happen in call order, so a buffer may be passed again (alternating two buffer pairs lets
+ * the caller read one frame while the next is copied).  Needs a non-default solver stream. */
+CRB200_API int CrB200SolverAdvanceAsync(CrB200SolverHandle solver, float dt, CrB200Float4 *positionMassHost,
+                                        CrB200Float4 *velocityHost, int *outSubsteps);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Setters and binders (MpmSolver, mpm_solver.h:80-184; MpmSolverBase, mpm_solver_base.h)      */
 /* ------------------------------------------------------------------------------------------ */
