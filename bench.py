@@ -438,6 +438,8 @@ def run_adjoint(args, rank, world, local):
     dev = f"cuda:{local}"
     torch.cuda.set_device(local)
     T, caps, K = 200, (50, 100, 150, 200), 20
+    if args.quick:  # short run for profiler launch lists: 40 substeps, the single cube only
+        T, caps, K = 40, (20, 40), 20
 
     def cube(seed):
         return scenes.material_cube(seed=seed, E=8e3, nu=0.25, drop=0.01, v0=(0.0, -1.0, 0.0))
@@ -476,7 +478,7 @@ def run_adjoint(args, rank, world, local):
                     backward_over_plain_forward=bwd / plain, grad_E_sign_check=float(gl.sum()))
 
     single = measure(cb.DeviceScene(cube(1005), device=dev), None)
-    batch = measure(cb.DeviceBatch([cube(2000 + s) for s in range(64)], device=dev), None)
+    batch = None if args.quick else measure(cb.DeviceBatch([cube(2000 + s) for s in range(64)], device=dev), None)
     n = single["particles"]
     value = n * T / (single["backward_ms"] / 1e3)
     return {

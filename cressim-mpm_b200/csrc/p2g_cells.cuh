@@ -422,6 +422,13 @@ namespace crb200
                         nid = sortedIds[start + q + 1];
                         loadRecord(records, nid, nxt);
                     }
+                    if (q + 2 < runEnd)
+                    {
+                        // the record after next into L1 (no registers held for it)
+                        const float4 *ahead = records + 4ull * sortedIds[start + q + 2];
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(ahead));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(ahead + 2));
+                    }
                     const unsigned msk = slicers ? cutMasks[id] : 0u;
                     if (msk)
                         accumulateCell<Mode, true>(p, rec, msk, pass, acc);
