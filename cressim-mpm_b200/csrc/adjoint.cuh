@@ -691,30 +691,30 @@ namespace crb200
         float4 *bv = bx + n;
         float *bF = reinterpret_cast<float *>(bv + n);
         float *bC = bF + 9ull * n;
-        const unsigned stepN = gridDim.x * blockDim.x;
-        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stepN)
+        const unsigned stepN = gridDim.x * blockDim.x, t0 = blockIdx.x * blockDim.x + threadIdx.x;
+        // x and v (float4 items), then the 18 planes of F and C (float items): independent
+        // elements, so every thread has loads in flight
+        for (unsigned t = t0; t < 2u * n; t += stepN)
         {
+            const unsigned i = t < n ? t : t - n;
+            float4 *a = t < n ? x : v;
+            float4 *b = t < n ? bx : bv;
             if (load)
-            {
-                x[i] = bx[i];
-                v[i] = bv[i];
-#pragma unroll
-                for (int k = 0; k < 9; ++k)
-                {
-                    F[k * stride + i] = bF[(size_t)k * n + i];
-                    C[k * stride + i] = bC[(size_t)k * n + i];
-                }
-            }
+                a[i] = b[i];
             else
+                b[i] = a[i];
+        }
+#pragma unroll 1
+        for (int plane = 0; plane < 18; ++plane)
+        {
+            float *a = plane < 9 ? F + (size_t)plane * stride : C + (size_t)(plane - 9) * stride;
+            float *b = plane < 9 ? bF + (size_t)plane * n : bC + (size_t)(plane - 9) * n;
+            for (unsigned i = t0; i < n; i += stepN)
             {
-                bx[i] = x[i];
-                bv[i] = v[i];
-#pragma unroll
-                for (int k = 0; k < 9; ++k)
-                {
-                    bF[(size_t)k * n + i] = F[k * stride + i];
-                    bC[(size_t)k * n + i] = C[k * stride + i];
-                }
+                if (load)
+                    a[i] = b[i];
+                else
+                    b[i] = a[i];
             }
         }
         if (load)
@@ -736,7 +736,7 @@ namespace crb200
         const unsigned n = totalParticles();
         if (!n)
             return CRB200_OK;
-        k_stateCopy<<<std::min((n + 255) / 256, (unsigned)strideCtas), 256, 0, stream>>>(
+        k_stateCopy<<<std::min((n + 255) / 256, 2u * (unsigned)strideCtas), 256, 0, stream>>>(
             n, (unsigned)numMaxParticles, false, positionMass, velocity, F, Cm, dst, nullptr, 0u, nullptr, 0u, nullptr);
         CRB_LAUNCHED(1);
         return CRB200_OK;
@@ -746,7 +746,7 @@ namespace crb200
     {
         const unsigned n = totalParticles();
         const unsigned nodes = totalBlocks * 64u;
-        k_stateCopy<<<std::max(1u, std::min((std::max(n, nodes) + 255) / 256, (unsigned)strideCtas)), 256, 0, stream>>>(
+        k_stateCopy<<<std::max(1u, std::min((std::max(n, nodes) + 255) / 256, 2u * (unsigned)strideCtas)), 256, 0, stream>>>(
             n, (unsigned)numMaxParticles, true, positionMass, velocity, F, Cm, const_cast<unsigned char *>(src),
             blockCount, totalBlocks + 1, cellCount, nodes, &header->recordsValid);
         CRB_LAUNCHED(1);
