@@ -13,7 +13,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/mpm_kernels.cu", "csrc/capi.cu", "csrc/noalloc.cu"]
+SOURCES = ["csrc/mpm_kernels.cu", "csrc/capi.cu", "csrc/noalloc.cu", "csrc/sdf_builder.cu"]
 OUT = os.path.join(HERE, "libcrmpm_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

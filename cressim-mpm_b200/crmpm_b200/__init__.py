@@ -71,6 +71,19 @@ class BatchSceneDescC(C.Structure):
                 ("numParticles", C.c_uint), ("shapeOffset", C.c_int), ("numShapes", C.c_int)]
 
 
+class TriangleMeshC(C.Structure):
+    """CrB200TriangleMesh (include/crmpm_b200.h)."""
+
+    _fields_ = [("points", C.c_void_p), ("triangles", C.c_void_p), ("numPoints", C.c_int), ("numTriangles", C.c_int)]
+
+
+class SdfDescC(C.Structure):
+    """CrB200SdfDesc (include/crmpm_b200.h)."""
+
+    _fields_ = [("cellSize", C.c_float), ("fatten", C.c_float), ("slicerSpineArea", C.c_float * 4),
+                ("boundingSize", C.c_float * 3), ("lowerBound", C.c_float * 3), ("sdfDimension", C.c_int * 3)]
+
+
 _lib = None
 
 
@@ -134,6 +147,9 @@ def lib() -> C.CDLL:
         "CrB200SolverAdjointRecord": (i, [vp, i, i, i, vp, vp]),
         "CrB200SolverAutotune": (i, [vp, i, vp]),
         "CrB200SolverAdjointBackward": (i, [vp, vp, vp, vp, vp]),
+        "CrB200SdfPrecomputeDesc": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC)]),
+        "CrB200SdfCompute": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC), vp, i, vp]),
+        "CrB200SdfComputeMod": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC), vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -159,6 +175,68 @@ def check(rc: int, what: str = "") -> None:
 
 def kernel_launch_count() -> int:
     return int(lib().CrB200GetKernelLaunchCount())
+
+
+class SdfGrid:
+    """An SDF grid built on the GPU: ``data`` is a torch float32 tensor [nz, ny, nx, 4] on the device
+    (gradient xyz, distance w; the flat layout the solvers' gradientSignedDistance arrays hold),
+    ``dims`` (nx, ny, nz), ``lower`` the position of node (0, 0, 0), ``cell`` the node spacing."""
+
+    def __init__(self, data, dims, lower, cell, size):
+        self.data, self.dims, self.lower, self.cell, self.size = data, dims, lower, cell, size
+
+    def host(self) -> np.ndarray:
+        """Flat float32 [nx * ny * nz, 4] copy in node order (x fastest)."""
+        return self.data.reshape(-1, 4).cpu().numpy()
+
+
+def _mesh_struct(points: np.ndarray, triangles: np.ndarray):
+    P = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    T = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+    m = TriangleMeshC(P.ctypes.data, T.ctypes.data, P.shape[0], T.shape[0])
+    return m, (P, T)
+
+
+def sdf_desc(points, triangles, cell_size: float, fatten: float = 0.0, spine=None) -> SdfDescC:
+    """SdfBuilder::precomputeSdfDesc (src/geometry_utils/sdf_builder.cpp:84-103) via
+    CrB200SdfPrecomputeDesc: the grid the reference lays over the mesh."""
+    m, keep = _mesh_struct(points, triangles)
+    d = SdfDescC()
+    d.cellSize = float(cell_size)
+    d.fatten = float(fatten)
+    sp = (float("nan"), 0.0, 0.0, 0.0) if spine is None else tuple(float(v) for v in spine)
+    d.slicerSpineArea = (C.c_float * 4)(*sp)
+    check(lib().CrB200SdfPrecomputeDesc(C.byref(d), C.byref(m)), "CrB200SdfPrecomputeDesc")
+    del keep
+    return d
+
+
+def build_sdf(points, triangles, cell_size: float, fatten: float = 0.0, normalize: bool = True,
+              slicer: bool = False, spine=None, device=None, out=None, stream: int | None = None) -> SdfGrid:
+    """Build the SDF grid of a triangle mesh on the GPU, as the reference's factory does when it
+    creates an eTriangleMesh geometry (computeSdf + computeSdfGradient) or, with ``slicer``, an
+    eTriangleMeshSlicer geometry (computeModSdf + computeSdfGradient + postProcessModSdfGradient,
+    spine plane ``spine`` = (nx, ny, nz, d) or None).  ``out``: optional device tensor of
+    nx * ny * nz * 4 float32 to write into (e.g. a slice of a scene's SDF data array)."""
+    import torch
+
+    d = sdf_desc(points, triangles, cell_size, fatten, spine)
+    nx, ny, nz = (int(v) for v in d.sdfDimension)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if out is None:
+        out = torch.empty((nz, ny, nx, 4), dtype=torch.float32, device=dev)
+    elif out.numel() != nx * ny * nz * 4 or out.dtype != torch.float32 or not out.is_contiguous():
+        raise CrmpmError("build_sdf: `out` must be a contiguous float32 tensor of nx * ny * nz * 4 elements")
+    m, keep = _mesh_struct(points, triangles)
+    st = C.c_void_p(stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream)
+    if slicer:
+        check(lib().CrB200SdfComputeMod(C.byref(d), C.byref(m), C.c_void_p(out.data_ptr()), st), "CrB200SdfComputeMod")
+    else:
+        check(lib().CrB200SdfCompute(C.byref(d), C.byref(m), C.c_void_p(out.data_ptr()), int(bool(normalize)), st),
+              "CrB200SdfCompute")
+    del keep
+    return SdfGrid(out, (nx, ny, nz), tuple(float(v) for v in d.lowerBound), float(d.cellSize),
+                   tuple(float(v) for v in d.boundingSize))
 
 
 class GpuSolver:

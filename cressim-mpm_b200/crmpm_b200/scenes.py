@@ -452,6 +452,45 @@ def contact_scene(kind: str, seed: int = 1010, solver: int = SOLVER_MLS, dt: flo
                  np.array([0, -9.81, 0], np.float32), 10, contact_model, pm, vel, mp, mt, mask, st, f"contact_{kind}")
 
 
+def mesh_contact_scene(dims, lower, cell: float, values=None, slicer: bool = False, spine=None, seed: int = 1012,
+                       dt: float = 2e-4):
+    """The contact cube of ``contact_scene`` against a triangle-mesh geometry whose SDF grid
+    (``dims``, ``lower``, ``cell``; ``values`` float32 [nx*ny*nz, 4] or zeros to fill later) was
+    built from a mesh: a rigid eTriangleMesh under the cube, or with ``slicer`` an
+    eTriangleMeshSlicer blade in the pose of the "mesh_slicer" kind (spine plane ``spine``, stored
+    one element before the grid as the reference's factory does).  Returns (scene, grid offset
+    into the scene's SDF data array)."""
+    cell_p = 0.02
+    h = 0.08
+    pos = jittered_box((-h, 0.12 - h, -h), (h, 0.12 + h, h), cell_p, 8, seed)
+    lam, mu = lame(2e4, 0.3)
+    pm, vel, mp, mt, mask = _particles(pos, 1000.0 * cell_p ** 3 / 8, (lam, mu, 0, 0), MAT_NEOHOOKEAN)
+    vel[:, 1] = -1.0
+    n = int(np.prod(dims))
+    vals = np.zeros((n, 4), np.float32) if values is None else np.asarray(values, np.float32).reshape(n, 4)
+    st = ShapeTable.empty()
+    kin = dict(smooth=cell_p, drag=0.8, friction=0.3)
+    if not slicer:
+        off, sid = st.add_sdf_block(dims, lower, cell, vals)
+        g = st.add_geometry(GEOM_TRIANGLE_MESH, (int_bits(off), int_bits(sid), int_bits(n), 0))
+        st.add_shape(g, SHAPE_STATIC, (0.0, 0.0, 0.01), **kin)
+        grid_off = off
+    else:
+        sp = np.asarray([(np.nan, 0.0, 0.0, 0.0) if spine is None else spine], np.float32)
+        off, sid = st.add_sdf_block(dims, lower, cell, vals, header=sp)
+        g = st.add_geometry(GEOM_TRIANGLE_MESH_SLICER, (int_bits(off), int_bits(sid), int_bits(n + 1), 0))
+        c = math.cos(math.pi / 4)
+        st.add_shape(g, SHAPE_KINEMATIC, (0.003, 0.12, 0.0), rotation=(0, 0, c, c), smooth=0.0, drag=1.0, friction=0.0,
+                     fatten=0.002, lin_vel=(0, -0.2, 0))
+        gp = st.add_geometry(GEOM_PLANE, (0, 0, 0, 0))
+        st.add_shape(gp, SHAPE_STATIC, (0, 0.0, 0), **kin)
+        grid_off = off + 1
+    sc = Scene(SOLVER_MLS, np.array([-0.3, -0.2, -0.3], np.float32), np.array([0.3, 0.4, 0.3], np.float32), cell_p, dt,
+               np.array([0, -9.81, 0], np.float32), 10, 0, pm, vel, mp, mt, mask, st,
+               "mesh_slicer_built" if slicer else "trimesh_built")
+    return sc, grid_off
+
+
 # Geometry types whose params (x, y) are (offset into the SDF data, SDF id) as int bits.
 _SDF_GEOMS = (GEOM_TRIANGLE_MESH, GEOM_TRIANGLE_MESH_SLICER, GEOM_CONNECTED_LINE_SEGMENTS)
 

@@ -393,6 +393,60 @@ typedef struct CrB200NoAllocStep {
  * is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
 CRB200_API int CrB200MlsSubstepNoAlloc(const CrB200NoAllocStep *step, void *stream);
 
+/* ------------------------------------------------------------------------------------------ */
+/* Triangle-mesh SDF grids built on the GPU (crmpm::SdfBuilder,                                */
+/* include/geometry_utils/sdf_builder.h:46-98, src/geometry_utils/sdf_builder.cpp:84-368)     */
+/* ------------------------------------------------------------------------------------------ */
+
+/* crmpm::TriangleMesh (include/geometry_utils/triangle_mesh.h:39-46): HOST arrays, points as
+ * numPoints x 3 floats, triangles as numTriangles x 3 vertex indices. */
+typedef struct CrB200TriangleMesh {
+    const float *points;
+    const unsigned int *triangles;
+    int numPoints;
+    int numTriangles;
+} CrB200TriangleMesh;
+
+/* crmpm::SdfDesc (include/geometry_utils/sdf_builder.h:46-66).  The caller sets cellSize, fatten
+ * and (slicer meshes only) slicerSpineArea, whose x is NaN when the slicer has no spine plane;
+ * CrB200SdfPrecomputeDesc fills in the rest. */
+typedef struct CrB200SdfDesc {
+    float cellSize;
+    float fatten;
+    CrB200Float4 slicerSpineArea;
+    float boundingSize[3];
+    float lowerBound[3];
+    int sdfDimension[3];
+} CrB200SdfDesc;
+
+/* SdfBuilder::precomputeSdfDesc (sdf_builder.cpp:84-103): the grid the reference lays over a mesh.
+ * Its box is the union of the triangles' boxes, each enlarged by 1e-4 (winding_number.h:145-156),
+ * then by `fatten`; like the reference's, each triangle box also contains the origin, because its
+ * corners start at (0, 0, 0) before the vertices are included.  sdfDimension = int(size / cell + 1)
+ * per axis.  Host only. */
+CRB200_API int CrB200SdfPrecomputeDesc(CrB200SdfDesc *desc, const CrB200TriangleMesh *mesh);
+
+/* SdfBuilder::computeSdf followed by computeSdfGradient (sdf_builder.cpp:105-161, 231-340), the
+ * sequence of SimulationFactoryImpl::createGeometry for eTriangleMesh
+ * (simulation_factory_impl.cpp:630-641).  Writes sdfDimension[0] x [1] x [2] float4 nodes (x
+ * fastest) at gradientSignedDistance (DEVICE pointer): w = distance to the closest point on the
+ * mesh, negative where the winding number of the mesh exceeds 0.5; xyz = its finite-difference
+ * gradient, normalised when normalizeGradient is nonzero.  `desc` must come from
+ * CrB200SdfPrecomputeDesc for the same mesh; every axis needs at least 2 nodes.  Enqueued on
+ * `stream` (NULL = legacy default stream); the mesh arrays may be reused when the call returns. */
+CRB200_API int CrB200SdfCompute(const CrB200SdfDesc *desc, const CrB200TriangleMesh *mesh,
+                                CrB200Float4 *gradientSignedDistance, int normalizeGradient, void *stream);
+
+/* The slicer variant: SdfBuilder::computeModSdf, computeSdfGradient (normalised) and
+ * postProcessModSdfGradient (sdf_builder.cpp:163-229, 231-340, 342-367), the sequence of
+ * createGeometry for eTriangleMeshSlicer (simulation_factory_impl.cpp:669-684).  w = unsigned
+ * distance; a node whose closest point lies on a boundary edge or boundary vertex of the mesh (an
+ * edge with fewer than two triangles) is off the mesh and gets NaN in all four components, unless
+ * desc->slicerSpineArea (x not NaN) puts it on the positive side of the spine plane.  The spine
+ * plane itself, which the reference stores one element before the grid, is the caller's to write. */
+CRB200_API int CrB200SdfComputeMod(const CrB200SdfDesc *desc, const CrB200TriangleMesh *mesh,
+                                   CrB200Float4 *gradientSignedDistance, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -352,3 +352,75 @@ def sdf_query(kind: str, geom_type: int, params0, st, pts: np.ndarray, prec: int
         sp = np.zeros(n, np.int32)
         lib.orc_sdf_query(prec, geom_type, _p(p0), C.byref(hs.sdf), n, _p(lp), _p(out), _p(tan), _p(sp))
     return out, tan, sp
+
+
+# ---------------------------------------------------------------------------------------------
+# Triangle-mesh SDF grids: the reference's own builder (oracle/_ref/libref_sdf.so) and the
+# restatement (sdf_oracle.cpp in oracle/liboracle.so)
+# ---------------------------------------------------------------------------------------------
+
+REF_SDF_LIB = os.path.join(HERE, "_ref", "libref_sdf.so")
+_ref_sdf_lib = None
+
+
+def ref_sdf_available() -> bool:
+    return os.path.exists(REF_SDF_LIB)
+
+
+def _mesh(points, triangles):
+    P = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    T = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+    return P, T
+
+
+def _spine(spine):
+    return np.asarray((np.nan, 0, 0, 0) if spine is None else spine, np.float32)
+
+
+def ref_sdf(points, triangles, cell: float, fatten: float = 0.0, normalize: bool = True, slicer: bool = False,
+            spine=None):
+    """(dims, lower, grid [nx*ny*nz, 4]) from the reference's SdfBuilder run on the host."""
+    global _ref_sdf_lib
+    if _ref_sdf_lib is None:
+        lib = C.CDLL(REF_SDF_LIB)
+        lib.ref_sdf_desc.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                     C.c_void_p]
+        lib.ref_sdf_build.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_int,
+                                      C.c_void_p]
+        lib.ref_sdf_build_mod.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_float, C.c_float,
+                                          C.c_void_p, C.c_void_p]
+        _ref_sdf_lib = lib
+    L = _ref_sdf_lib
+    P, T = _mesh(points, triangles)
+    dims = np.zeros(3, np.int32)
+    lower = np.zeros(3, np.float32)
+    L.ref_sdf_desc(_p(P), P.shape[0], _p(T), T.shape[0], cell, fatten, _p(dims), _p(lower))
+    n = int(np.prod(dims.astype(np.int64)))
+    out = np.zeros((n, 4), np.float32)
+    if slicer:
+        L.ref_sdf_build_mod(_p(P), P.shape[0], _p(T), T.shape[0], cell, fatten, _p(_spine(spine)), _p(out))
+    else:
+        L.ref_sdf_build(_p(P), P.shape[0], _p(T), T.shape[0], cell, fatten, int(normalize), _p(out))
+    return tuple(int(v) for v in dims), lower, out
+
+
+def port_sdf(points, triangles, cell: float, fatten: float = 0.0, normalize: bool = True, slicer: bool = False,
+             spine=None):
+    """(dims, lower, size, grid [nx*ny*nz, 4]) from the restatement (sdf_oracle.cpp)."""
+    L = _load_port()
+    if not getattr(L, "_sdf_sig", False):
+        L.oracle_sdf_desc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]
+        L.oracle_sdf_build.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_float,
+                                       C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        L._sdf_sig = True
+    P, T = _mesh(points, triangles)
+    dims = np.zeros(3, np.int32)
+    lower = np.zeros(3, np.float32)
+    size = np.zeros(3, np.float32)
+    L.oracle_sdf_desc(_p(P), _p(T), T.shape[0], cell, fatten, _p(dims), _p(lower), _p(size))
+    out = np.zeros((int(np.prod(dims.astype(np.int64))), 4), np.float32)
+    sp = _spine(spine)
+    L.oracle_sdf_build(_p(P), P.shape[0], _p(T), T.shape[0], _p(dims), _p(lower), cell, int(slicer), _p(sp),
+                       int(normalize), _p(out))
+    return tuple(int(v) for v in dims), lower, size, out

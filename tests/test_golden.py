@@ -30,7 +30,7 @@ def scene_from(z):
 
 
 CASES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLD, "*.npz"))
-               if not os.path.basename(p).startswith(("svd3", "sdf_queries")))
+               if not os.path.basename(p).startswith(("svd3", "sdf_queries", "meshsdf_")))
 
 
 def test_fixtures_present():
