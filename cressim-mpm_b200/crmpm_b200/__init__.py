@@ -150,6 +150,7 @@ def lib() -> C.CDLL:
         "CrB200SdfPrecomputeDesc": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC)]),
         "CrB200SdfCompute": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC), vp, i, vp]),
         "CrB200SdfComputeMod": (i, [C.POINTER(SdfDescC), C.POINTER(TriangleMeshC), vp, vp]),
+        "CrB200SdfGetLastKernelTime": (i, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -237,6 +238,14 @@ def build_sdf(points, triangles, cell_size: float, fatten: float = 0.0, normaliz
     del keep
     return SdfGrid(out, (nx, ny, nz), tuple(float(v) for v in d.lowerBound), float(d.cellSize),
                    tuple(float(v) for v in d.boundingSize))
+
+
+def sdf_last_kernel_ms() -> tuple[float, float]:
+    """GPU times (distance kernel, gradient kernel) in ms of the last build_sdf on this thread
+    (CrB200SdfGetLastKernelTime)."""
+    ms = (C.c_float * 2)()
+    check(lib().CrB200SdfGetLastKernelTime(ms), "CrB200SdfGetLastKernelTime")
+    return float(ms[0]), float(ms[1])
 
 
 class GpuSolver:

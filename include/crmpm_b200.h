@@ -447,6 +447,12 @@ CRB200_API int CrB200SdfCompute(const CrB200SdfDesc *desc, const CrB200TriangleM
 CRB200_API int CrB200SdfComputeMod(const CrB200SdfDesc *desc, const CrB200TriangleMesh *mesh,
                                    CrB200Float4 *gradientSignedDistance, void *stream);
 
+/* GPU times in ms of the two kernels of the most recent CrB200SdfCompute / CrB200SdfComputeMod
+ * call made on this host thread: outMs[0] the distance (and sign or off-mesh flag) kernel, outMs[1]
+ * the gradient kernel; waits for them.  Host-side preparation and the mesh upload are not
+ * included.  No counterpart in the reference. */
+CRB200_API int CrB200SdfGetLastKernelTime(float outMs[2]);
+
 #ifdef __cplusplus
 }
 #endif

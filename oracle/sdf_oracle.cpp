@@ -9,8 +9,8 @@
 //     (sdf_builder.cpp:142-143);
 //   - sign: winding number > 0.5 (sdf_builder.cpp:147-153), here the exact sum over all
 //     triangles of the term of evaluateExact (winding_number.h:93-109);
-//   - slicer meshes: unsigned distance; off the mesh where a closest feature (within a relative
-//     1e-5 of the smallest squared distance) is a boundary vertex or boundary edge
+//   - slicer meshes: unsigned distance; off the mesh where the closest feature of any triangle
+//     within a relative 1e-5 of the smallest squared distance is a boundary vertex or boundary edge
 //     (aabb_tree.cpp:523-625, 724-760), on the mesh on the positive side of the spine plane
 //     (sdf_builder.cpp:217-226); NaN nodes off the mesh after the gradient (sdf_builder.cpp:342-367);
 //   - gradient: computeSdfGradient (sdf_builder.cpp:231-340).
@@ -161,16 +161,20 @@ extern "C"
                         V h;
                         int f;
                         const float d2 = closest(q, a, b, c, h, f);
-                        if (mod)
-                        {
-                            const bool out = f < 6 && ((bits[i] >> f) & 1u);
-                            if (d2 < best * (1.f - 1e-5f))
-                                off = out;
-                            else if (d2 <= best * (1.f + 1e-5f))
-                                off = off || out;
-                        }
                         if (d2 < best)
                             best = d2, cp = h;
+                    }
+                    if (mod)
+                    {
+                        // every triangle within a relative 1e-5 of the closest squared distance
+                        const float tie = best * (1.f + 1e-5f);
+                        for (int i = 0; i < nt && !off; ++i)
+                        {
+                            V h;
+                            int f;
+                            const float d2 = closest(q, P(tris[3 * i]), P(tris[3 * i + 1]), P(tris[3 * i + 2]), h, f);
+                            off = d2 <= tie && f < 6 && ((bits[i] >> f) & 1u);
+                        }
                     }
                     const V e = cp - q;
                     const float d = std::sqrt(dot(e, e));
