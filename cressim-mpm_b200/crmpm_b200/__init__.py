@@ -31,6 +31,7 @@ STATUS_NAN_STATE = 0x1
 STATUS_BLOCK_OVERFLOW = 0x2
 STATUS_OUT_OF_DOMAIN = 0x4
 OPT_PHASE_TIMING = 3
+OPT_DETERMINISTIC_COUPLING = 4
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 
 

@@ -536,6 +536,11 @@ extern "C"
         SOLVER_OR_FAIL(solver);
         if (option == CRB200_OPT_PHASE_TIMING)
             s->phaseTiming = value != 0;
+        else if (option == CRB200_OPT_DETERMINISTIC_COUPLING)
+        {
+            if (int rc = s->setDeterministicCoupling(value != 0))
+                return rc;
+        }
         else
             return bad("CrB200SolverSetOption: unknown option");
         s->configVersion++;

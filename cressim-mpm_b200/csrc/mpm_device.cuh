@@ -39,7 +39,8 @@ namespace crb200
     struct __align__(16) ShapeRec
     {
         float4 pos, rot, invScale, linVel, angVel, params0, gparams, comInvMass, inertia0, inertia1, cull;
-        int kind, gtype, id, pad;
+        int kind, gtype, id;
+        int dynSlot; // rank among the scene's dynamic shapes (deterministic coupling), -1 otherwise
     };
 
     struct SdfPtrs
@@ -460,7 +461,7 @@ namespace crb200
         r.kind = sh.type[id];
         r.gtype = ge.type[gid];
         r.id = id;
-        r.pad = 0;
+        r.dynSlot = -1;
         const float maxIsc = fmaxf(fabsf(r.invScale.x), fmaxf(fabsf(r.invScale.y), fabsf(r.invScale.z)));
         const bool analytic = r.gtype == G_BOX || r.gtype == G_SPHERE || r.gtype == G_PLANE || r.gtype == G_CAPSULE;
         const float band = r.params0.x + r.params0.w, pband = r.params0.w;
@@ -481,16 +482,60 @@ namespace crb200
         return f;
     }
 
+    constexpr int kDetSlots = 4; // dynamic shapes whose coupling is reduced deterministically
+
+    // Where the grid contact puts the momentum it exchanges with a dynamic shape.
+    // CoupleAtomic: float atomics into the shape's force / torque, in arrival order, as the
+    // reference does (mpm_rigid_contact.h:59-82, 380-389).
+    struct CoupleAtomic
+    {
+        float4 *force, *torque;
+        __device__ __forceinline__ void add(const ShapeRec &r, V3 mom, V3 tq)
+        {
+            atomicAdd(&force[r.id].x, mom.x);
+            atomicAdd(&force[r.id].y, mom.y);
+            atomicAdd(&force[r.id].z, mom.z);
+            atomicAdd(&torque[r.id].x, tq.x);
+            atomicAdd(&torque[r.id].y, tq.y);
+            atomicAdd(&torque[r.id].z, tq.z);
+        }
+    };
+
+    // CoupleRow: this thread's row of per-slot sums (force xyz, torque xyz for each of the first
+    // kDetSlots dynamic shapes) in shared memory, reduced later in a fixed order; further dynamic
+    // shapes fall back to atomics.
+    struct CoupleRow
+    {
+        float *row; // kDetSlots * 6 floats
+        CoupleAtomic spill;
+        bool any; // some momentum went into the row
+        __device__ __forceinline__ void add(const ShapeRec &r, V3 mom, V3 tq)
+        {
+            if (r.dynSlot < 0 || r.dynSlot >= kDetSlots)
+            {
+                spill.add(r, mom, tq);
+                return;
+            }
+            any = true;
+            float *q = row + 6 * r.dynSlot;
+            q[0] += mom.x;
+            q[1] += mom.y;
+            q[2] += mom.z;
+            q[3] += tq.x;
+            q[4] += tq.y;
+            q[5] += tq.z;
+        }
+    };
+
     // resolveRigidCollision (mpm_rigid_contact.h:101-399).
     //   isParticle = false: grid node with velocity vel (mass m) evaluated at pos; contact inside
     //       the smooth distance, separating nodes skipped, Coulomb-like friction, drag, rigid
     //       velocity, line/arc tangent restriction, dynamic coupling (kinematic or effective mass).
     //   isParticle = true: positional push-out only (lines and arcs skipped).
     //   mask: shapes to consider (bit s = shape s); shapes outside it are known not to reach pos.
-    template <bool IsParticle>
+    template <bool IsParticle, class Couple = CoupleAtomic>
     __device__ __forceinline__ void rigidContact(V3 &vel, float m, V3 &pos, const ShapeRec *sh, int num, const SdfPtrs &sdf,
-                                                 bool effMass, float4 *coupleForce, float4 *coupleTorque,
-                                                 unsigned long long mask = ~0ull)
+                                                 bool effMass, Couple &couple, unsigned long long mask = ~0ull)
     {
         unsigned long long left = mask & (num >= 64 ? ~0ull : ((1ull << num) - 1ull));
         while (left)
@@ -561,13 +606,7 @@ namespace crb200
                         const V3 tot = normal * Jn + impT;
                         resp = vel + tot * invMassGrid;
                         const V3 mom = tot * -1.f;
-                        const V3 tq = cross(rr, mom);
-                        atomicAdd(&coupleForce[r.id].x, mom.x);
-                        atomicAdd(&coupleForce[r.id].y, mom.y);
-                        atomicAdd(&coupleForce[r.id].z, mom.z);
-                        atomicAdd(&coupleTorque[r.id].x, tq.x);
-                        atomicAdd(&coupleTorque[r.id].y, tq.y);
-                        atomicAdd(&coupleTorque[r.id].z, tq.z);
+                        couple.add(r, mom, cross(rr, mom));
                     }
                 }
             }
@@ -585,13 +624,7 @@ namespace crb200
                 if (!effMass && r.kind == S_DYNAMIC)
                 {
                     const V3 mom = (vel - resp) * m;
-                    const V3 tq = cross(pos - v3(r.pos), mom);
-                    atomicAdd(&coupleForce[r.id].x, mom.x);
-                    atomicAdd(&coupleForce[r.id].y, mom.y);
-                    atomicAdd(&coupleForce[r.id].z, mom.z);
-                    atomicAdd(&coupleTorque[r.id].x, tq.x);
-                    atomicAdd(&coupleTorque[r.id].y, tq.y);
-                    atomicAdd(&coupleTorque[r.id].z, tq.z);
+                    couple.add(r, mom, cross(pos - v3(r.pos), mom));
                 }
             }
             vel = resp;

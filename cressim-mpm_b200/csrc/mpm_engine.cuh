@@ -220,6 +220,10 @@ namespace crb200
         float4 *adjForce = nullptr, *adjTorque = nullptr;      // coupling output of recomputed substeps
         int sortParticles(const StepParams &p, bool ignoreMask);
         void gatherShapes(cudaStream_t s);
+        bool detCoupling = false;            // CRB200_OPT_DETERMINISTIC_COUPLING
+        float4 *detPartials = nullptr;       // per block and dynamic slot: force, torque partial sums
+        unsigned *detMask = nullptr;         // bit per block: detPartials holds sums for it
+        int setDeterministicCoupling(bool on);
         cudaStream_t sideStream = nullptr; // shape gather / cut masks beside the sort chain
         cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     };

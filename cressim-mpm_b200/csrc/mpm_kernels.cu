@@ -222,15 +222,26 @@ namespace crb200
                                    CrB200GeometryData ge, ShapeRec *__restrict__ out)
     {
         __shared__ int flags;
+        __shared__ unsigned long long dynamic; // single scene: bit s = shape s is dynamic
         const int scene = blockIdx.x;
         const StepParams &sp = sc.numScenes > 1 ? sc.params[scene] : p;
         if (threadIdx.x == 0)
+        {
             flags = 0;
+            dynamic = 0ull;
+        }
+        __syncthreads();
+        if (sc.numScenes == 1)
+            for (int s = threadIdx.x; s < sp.numShapes && s < 64; s += blockDim.x)
+                if (sh.type[shapeIds[sp.shapeBegin + s]] == S_DYNAMIC)
+                    atomicOr(&dynamic, 1ull << s);
         __syncthreads();
         for (int s = threadIdx.x; s < sp.numShapes; s += blockDim.x)
         {
             const int t = sp.shapeBegin + s;
-            const ShapeRec r = makeShapeRec(shapeIds[t], sh, ge);
+            ShapeRec r = makeShapeRec(shapeIds[t], sh, ge);
+            if (sc.numScenes == 1 && s < 64 && r.kind == S_DYNAMIC)
+                r.dynSlot = __popcll(dynamic & ((1ull << s) - 1ull)); // rank among the dynamic shapes
             out[t] = r;
             atomicOr(&flags, shapeFlagsOf(r));
         }
@@ -533,7 +544,11 @@ namespace crb200
     // 7. Grid update over touched blocks (mls_mpm_algorithm.h:243-294 and its PB / standard twins).
     //    Multi: the touched blocks belong to many scenes; each block reads its scene's parameters
     //    and shapes from global memory (single scene: kernel arguments and shared memory).
-    template <bool Multi>
+    //    Det: coupling momentum of the first kDetSlots dynamic shapes is summed per 4x4x4 block in a
+    //    fixed order and written to detPartials[(block * kDetSlots + slot) * 2 + {0: force, 1: torque}]
+    //    (bit `block` of detMask set) for k_coupleReduce, instead of float atomics into the shapes'
+    //    force and torque.
+    template <bool Multi, bool Det>
     __global__ void __launch_bounds__(256) k_gridUpdate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                         const unsigned *__restrict__ touchedList,
                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -541,10 +556,12 @@ namespace crb200
                                                         float4 *__restrict__ gridV, float4 *coupleForce,
                                                         float4 *coupleTorque, bool clearA,
                                                         unsigned long long *__restrict__ blockShapeMask,
-                                                        float4 *__restrict__ saveA, float4 *__restrict__ saveV)
+                                                        float4 *__restrict__ saveA, float4 *__restrict__ saveV,
+                                                        float4 *__restrict__ detPartials, unsigned *__restrict__ detMask)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
+        __shared__ float sCouple[Det ? 256 : 1][kDetSlots * 6]; // Det: one row of coupling sums per thread
         if (threadIdx.x == 0)
             sTouched = 0;
         if (!Multi && p0.numShapes > 0)
@@ -553,86 +570,184 @@ namespace crb200
         const unsigned nT = hdr->numTouchedBlocks;
         const bool withForce = p0.solverType == CRB200_SOLVER_GPU_STANDARD;
         const unsigned perCta = blockDim.x / 64;
+        using Couple = typename std::conditional<Det, CoupleRow, CoupleAtomic>::type;
+        if constexpr (Det)
+            for (int c = 0; c < kDetSlots * 6; ++c)
+                sCouple[threadIdx.x][c] = 0.f;
         for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
         {
             const unsigned bi = base + threadIdx.x / 64;
-            if (bi >= nT)
-                continue;
-            const unsigned b = touchedList[bi];
-            const StepParams &p = Multi ? sc.params[sceneOfBlock(sc, b)] : p0;
-            const GridGeom &g = p.g;
-            const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
-            const unsigned l = threadIdx.x & 63;
-            const unsigned lb = b - g.blockBase;
-            const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
-            // shapes that can reach this block's region: one test per shape and warp instead of
-            // one per node, and the particle mask for G2P / PB-MPM integration
-            const BlockRegion region = blockRegion(g, bx, by, bz);
-            unsigned long long nodeMask = ~0ull;
-            if (p.numShapes > 0)
+            Couple couple;
+            if constexpr (Det)
+                couple = CoupleRow{sCouple[threadIdx.x], CoupleAtomic{coupleForce, coupleTorque}, false};
+            else
+                couple = CoupleAtomic{coupleForce, coupleTorque};
+            unsigned b = 0;
+            // one node of block touchedList[bi]; leaves early where the reference's update returns
+            do
             {
-                V3 bc;
-                float bR;
-                regionBall(region, bc, bR);
-                unsigned long long partMask;
-                regionShapeMasks(shp, p.numShapes, bc, bR, nodeMask, partMask);
-                if (l == 0)
-                    blockShapeMask[b] = partMask;
-            }
-            const int i = 4 * bx + (l & 3), j = 4 * by + ((l >> 2) & 3), k = 4 * bz + (l >> 4);
-            if (!inGrid(g, i, j, k))
-                continue;
-            const unsigned a = b * 64u + l;
-            float4 acc = gridA[a];
-            if (clearA)
-                gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (saveA)
-                saveA[a] = acc; // the adjoint's tape of this substep's P2G grid
-            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (withForce)
-            {
-                f = gridF[a];
-                gridF[a] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            {
-                // nodes that received mass (roofline bookkeeping): a shared counter per CTA
-                const unsigned am = __activemask();
-                const unsigned hit = __ballot_sync(am, acc.w > 0.f);
-                if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1) && hit)
-                    atomicAdd(&sTouched, (unsigned)__popc(hit));
-            }
-            if (acc.w < p.cutoff)
-            {
-                gridV[a] = acc; // light nodes keep momentum, which G2P then reads (reference Q2)
+                if (bi >= nT)
+                    break;
+                b = touchedList[bi];
+                const StepParams &p = Multi ? sc.params[sceneOfBlock(sc, b)] : p0;
+                const GridGeom &g = p.g;
+                const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
+                const unsigned l = threadIdx.x & 63;
+                const unsigned lb = b - g.blockBase;
+                const int bx = lb % g.nb.x, by = (lb / g.nb.x) % g.nb.y, bz = lb / (g.nb.x * g.nb.y);
+                // shapes that can reach this block's region: one test per shape and warp instead of
+                // one per node, and the particle mask for G2P / PB-MPM integration
+                const BlockRegion region = blockRegion(g, bx, by, bz);
+                unsigned long long nodeMask = ~0ull;
+                if (p.numShapes > 0)
+                {
+                    V3 bc;
+                    float bR;
+                    regionBall(region, bc, bR);
+                    unsigned long long partMask;
+                    regionShapeMasks(shp, p.numShapes, bc, bR, nodeMask, partMask);
+                    if (l == 0)
+                        blockShapeMask[b] = partMask;
+                }
+                const int i = 4 * bx + (l & 3), j = 4 * by + ((l >> 2) & 3), k = 4 * bz + (l >> 4);
+                if (!inGrid(g, i, j, k))
+                    break;
+                const unsigned a = b * 64u + l;
+                float4 acc = gridA[a];
+                if (clearA)
+                    gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (saveA)
+                    saveA[a] = acc; // the adjoint's tape of this substep's P2G grid
+                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (withForce)
+                {
+                    f = gridF[a];
+                    gridF[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                {
+                    // nodes that received mass (roofline bookkeeping): a shared counter per CTA
+                    const unsigned am = __activemask();
+                    const unsigned hit = __ballot_sync(am, acc.w > 0.f);
+                    if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1) && hit)
+                        atomicAdd(&sTouched, (unsigned)__popc(hit));
+                }
+                if (acc.w < p.cutoff)
+                {
+                    gridV[a] = acc; // light nodes keep momentum, which G2P then reads (reference Q2)
+                    if (saveV)
+                        saveV[a] = acc;
+                    break;
+                }
+                if (withForce)
+                {
+                    acc.x += f.x * p.dt;
+                    acc.y += f.y * p.dt;
+                    acc.z += f.z * p.dt;
+                }
+                V3 v = v3(acc.x / acc.w, acc.y / acc.w, acc.z / acc.w);
+                V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z);
+                pos = pos + v * p.dt;
+                if (p.numShapes > 0)
+                    rigidContact<false>(v, acc.w, pos, shp, p.numShapes, sdf, p.contactModel == 1, couple,
+                                        region.contains(pos) ? nodeMask : ~0ull);
+                if (i < 2 || i > g.n.x - 3)
+                    v.x = 0.f;
+                if (j < 2 || j > g.n.y - 3)
+                    v.y = 0.f;
+                if (k < 2 || k > g.n.z - 3)
+                    v.z = 0.f;
+                gridV[a] = make_float4(v.x, v.y, v.z, acc.w);
                 if (saveV)
-                    saveV[a] = acc;
-                continue;
-            }
-            if (withForce)
+                    saveV[a] = make_float4(v.x, v.y, v.z, acc.w);
+            } while (false);
+            if constexpr (Det)
             {
-                acc.x += f.x * p.dt;
-                acc.y += f.y * p.dt;
-                acc.z += f.z * p.dt;
+                // block sums in a fixed order: thread c < 24 of each 64-thread group adds column c
+                // of the group's rows in row order, writes it and clears the column
+                if (__syncthreads_or(couple.any))
+                {
+                    const unsigned l = threadIdx.x & 63, g0 = threadIdx.x - l;
+                    if (l < kDetSlots * 6 && bi < nT)
+                    {
+                        float t = 0.f;
+                        for (int r = 0; r < 64; ++r)
+                        {
+                            t += sCouple[g0 + r][l];
+                            sCouple[g0 + r][l] = 0.f;
+                        }
+                        const int slot = l / 6, c = l % 6;
+                        float *dst = reinterpret_cast<float *>(&detPartials[((size_t)b * kDetSlots + slot) * 2 + c / 3]);
+                        dst[c % 3] = t;
+                        if (l == 0)
+                            atomicOr(&detMask[b >> 5], 1u << (b & 31)); // the block holds partials
+                    }
+                    __syncthreads();
+                }
             }
-            V3 v = v3(acc.x / acc.w, acc.y / acc.w, acc.z / acc.w);
-            V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z);
-            pos = pos + v * p.dt;
-            if (p.numShapes > 0)
-                rigidContact<false>(v, acc.w, pos, shp, p.numShapes, sdf, p.contactModel == 1, coupleForce, coupleTorque,
-                                    region.contains(pos) ? nodeMask : ~0ull);
-            if (i < 2 || i > g.n.x - 3)
-                v.x = 0.f;
-            if (j < 2 || j > g.n.y - 3)
-                v.y = 0.f;
-            if (k < 2 || k > g.n.z - 3)
-                v.z = 0.f;
-            gridV[a] = make_float4(v.x, v.y, v.z, acc.w);
-            if (saveV)
-                saveV[a] = make_float4(v.x, v.y, v.z, acc.w);
         }
         __syncthreads();
         if (threadIdx.x == 0 && sTouched)
             atomicAdd(&const_cast<SortHeader *>(hdr)->touchedNodes, sTouched);
+    }
+
+    // Deterministic coupling reduction (one CTA): the blocks flagged in detMask, each thread taking
+    // mask words t, t + 256, ... and their blocks in ascending order, then a fixed tree over the
+    // threads; the sums are added to the dynamic shapes' force and torque.  Mask words and partials
+    // are zeroed once read.
+    __global__ void __launch_bounds__(256) k_coupleReduce(unsigned numMaskWords, unsigned *__restrict__ detMask,
+                                                          float4 *__restrict__ detPartials,
+                                                          const ShapeRec *__restrict__ shapeTable, int numShapes,
+                                                          float4 *force, float4 *torque)
+    {
+        __shared__ float sSum[256][kDetSlots * 6 + 1];
+        float t[kDetSlots * 6];
+#pragma unroll
+        for (int c = 0; c < kDetSlots * 6; ++c)
+            t[c] = 0.f;
+        for (unsigned w = threadIdx.x; w < numMaskWords; w += blockDim.x)
+        {
+            unsigned m = detMask[w];
+            if (!m)
+                continue;
+            detMask[w] = 0u;
+            while (m)
+            {
+                const unsigned b = w * 32u + (unsigned)(__ffs(m) - 1);
+                m &= m - 1u;
+#pragma unroll
+                for (int s = 0; s < kDetSlots; ++s)
+                {
+                    const size_t e = ((size_t)b * kDetSlots + s) * 2;
+                    const float4 f = detPartials[e], q = detPartials[e + 1];
+                    t[6 * s + 0] += f.x, t[6 * s + 1] += f.y, t[6 * s + 2] += f.z;
+                    t[6 * s + 3] += q.x, t[6 * s + 4] += q.y, t[6 * s + 5] += q.z;
+                    detPartials[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    detPartials[e + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kDetSlots * 6; ++c)
+            sSum[threadIdx.x][c] = t[c];
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1)
+        {
+            if (threadIdx.x < (unsigned)h)
+                for (int c = 0; c < kDetSlots * 6; ++c)
+                    sSum[threadIdx.x][c] += sSum[threadIdx.x + h][c];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && force && torque)
+            for (int s = 0; s < numShapes; ++s)
+            {
+                const int slot = shapeTable[s].dynSlot;
+                if (slot < 0 || slot >= kDetSlots)
+                    continue;
+                const int id = shapeTable[s].id;
+                const float *v = sSum[0] + 6 * slot;
+                force[id].x += v[0], force[id].y += v[1], force[id].z += v[2];
+                torque[id].x += v[3], torque[id].y += v[4], torque[id].z += v[5];
+            }
     }
 
     // 8. G2P in particle order.  Mode 0 MLS (mls_mpm_algorithm.h:296-390), 1 PB
@@ -937,7 +1052,8 @@ namespace crb200
             int bx, by, bz;
             const unsigned blk = baseBlock(g, st, bx, by, bz);
             const bool near = blockRegion(g, bx, by, bz).contains(xn);
-            rigidContact<true>(vn, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr,
+            CoupleAtomic noCouple{nullptr, nullptr}; // particle push-out exchanges no momentum
+            rigidContact<true>(vn, x4.w, xn, shp, p.numShapes, sdf, false, noCouple,
                                near ? blockShapeMask[blk] : ~0ull);
         }
         M3 Fp, Mu;
@@ -1030,7 +1146,8 @@ namespace crb200
             int bx, by, bz;
             const unsigned blk = baseBlock(g, st, bx, by, bz);
             const bool near = st.finite && blockRegion(g, bx, by, bz).contains(xn);
-            rigidContact<true>(v, x4.w, xn, shp, p.numShapes, sdf, false, nullptr, nullptr,
+            CoupleAtomic noCouple{nullptr, nullptr}; // particle push-out exchanges no momentum
+            rigidContact<true>(v, x4.w, xn, shp, p.numShapes, sdf, false, noCouple,
                                near ? blockShapeMask[blk] : ~0ull);
         }
         M3 Fp, Cp, Mu;
@@ -1417,7 +1534,7 @@ namespace crb200
                 cudaEventDestroy(e);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, cellCount, blockCount, blockStart,
                         activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, cellStart,
-                        dParams, dParticleScene, dSceneFlags, blockShapeMask};
+                        dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -1437,6 +1554,27 @@ namespace crb200
             cudaEventDestroy(joinEvent);
         if (sideStream)
             cudaStreamDestroy(sideStream);
+    }
+
+    // Deterministic coupling: the block partial buffer (zeroed; the reduction keeps it zeroed).
+    int Solver::setDeterministicCoupling(bool on)
+    {
+        if (on && isBatch())
+        {
+            setLastError("deterministic coupling: not available on batch solvers");
+            return CRB200_ERR_UNSUPPORTED;
+        }
+        if (on && !detPartials)
+        {
+            const size_t bytes = (size_t)totalBlocks * kDetSlots * 2 * sizeof(float4);
+            const size_t maskBytes = (size_t)(totalBlocks + 31) / 32 * sizeof(unsigned);
+            CRB_CHECK(cudaMalloc(&detPartials, bytes));
+            CRB_CHECK(cudaMemset(detPartials, 0, bytes));
+            CRB_CHECK(cudaMalloc(&detMask, maskBytes));
+            CRB_CHECK(cudaMemset(detMask, 0, maskBytes));
+        }
+        detCoupling = on;
+        return CRB200_OK;
     }
 
     StepParams Solver::params() const
@@ -1655,13 +1793,28 @@ namespace crb200
             return CRB200_OK;
         };
         auto update = [&]() -> int {
-            k_gridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV,
-                                                             (recompute || adjReplay) ? adjForce : cf,
-                                                             (recompute || adjReplay) ? adjTorque : ct,
-                                                             !recompute || tapeActive >= 0,
-                                                             blockShapeMask, tapeActive >= 0 ? tapeSlot(tapeActive).gridA : nullptr,
-                                                             tapeActive >= 0 ? tapeSlot(tapeActive).gridV : nullptr);
-            CRB_LAUNCHED(1);
+            const bool det = detCoupling && !Multi && !(recompute || adjReplay) && detPartials != nullptr;
+            auto upd = [&](auto detTag) {
+                constexpr bool D = decltype(detTag)::value;
+                k_gridUpdate<Multi, D><<<updCtas, 256, 0, stream>>>(
+                    p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV, (recompute || adjReplay) ? adjForce : cf,
+                    (recompute || adjReplay) ? adjTorque : ct, !recompute || tapeActive >= 0, blockShapeMask,
+                    tapeActive >= 0 ? tapeSlot(tapeActive).gridA : nullptr,
+                    tapeActive >= 0 ? tapeSlot(tapeActive).gridV : nullptr, D ? detPartials : nullptr,
+                    D ? detMask : nullptr);
+            };
+            if (det)
+            {
+                upd(std::true_type{});
+                k_coupleReduce<<<1, 256, 0, stream>>>((totalBlocks + 31) / 32, detMask, detPartials, shapeTable, numShapes,
+                                                      cf, ct);
+                CRB_LAUNCHED(2);
+            }
+            else
+            {
+                upd(std::false_type{});
+                CRB_LAUNCHED(1);
+            }
             if (tapeActive >= 0)
             {
                 const TapeSlot ts = tapeSlot(tapeActive);

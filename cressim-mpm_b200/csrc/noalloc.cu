@@ -193,7 +193,10 @@ namespace crb200
             V3 v = v3(a.x / a.w, a.y / a.w, a.z / a.w);
             V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin) + v * dt;
             if (numShapes > 0)
-                rigidContact<false>(v, a.w, pos, sh, numShapes, sdf, contactModel == 1, coupleForce, coupleTorque);
+                {
+                    CoupleAtomic couple{coupleForce, coupleTorque};
+                    rigidContact<false>(v, a.w, pos, sh, numShapes, sdf, contactModel == 1, couple);
+                }
             if (i < 2 || i > g.nx - 3)
                 v.x = 0.f;
             if (j < 2 || j > g.ny - 3)
@@ -280,7 +283,10 @@ namespace crb200
                     fminf(fmaxf(xn.z, g.gmin.z), g.gmax.z));
             V3 vn = va;
             if (numShapes > 0)
-                rigidContact<true>(vn, x4.w, xn, sh, numShapes, sdf, false, nullptr, nullptr);
+                {
+                    CoupleAtomic noCouple{nullptr, nullptr};
+                    rigidContact<true>(vn, x4.w, xn, sh, numShapes, sdf, false, noCouple);
+                }
             Fp = matmul(Mu, Fp);
             xm[p] = make_float4(xn.x, xn.y, xn.z, x4.w);
             vel[p] = make_float4(vn.x, vn.y, vn.z, 0.f);

@@ -264,8 +264,15 @@ CRB200_API int CrB200SolverGetStatus(CrB200SolverHandle solver, unsigned int *ou
 CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
 
 /* Option switches: CRB200_OPT_PHASE_TIMING records CUDA events around the phases of every
- * substep (see CrB200SolverGetPhaseTimes); it disables CUDA-graph replay while on. */
+ * substep (see CrB200SolverGetPhaseTimes); it disables CUDA-graph replay while on.
+ * CRB200_OPT_DETERMINISTIC_COUPLING makes the momentum that grid contact exchanges with dynamic
+ * shapes (the force and torque accumulated into ShapeData, mpm_rigid_contact.h:59-82, 380-389)
+ * independent of thread scheduling: per 4x4x4 grid block in a fixed order, then over blocks in
+ * ascending order, instead of float atomics in arrival order.  Covers the first 4 dynamic shapes
+ * of a scene (later ones keep the atomics); single-scene solvers only (CRB200_ERR_UNSUPPORTED on a
+ * batch).  The first switch-on allocates 128 bytes per grid block. */
 #define CRB200_OPT_PHASE_TIMING 3
+#define CRB200_OPT_DETERMINISTIC_COUPLING 4
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the

@@ -90,6 +90,43 @@ def test_dynamic_coupling_force(kind):
     np.testing.assert_allclose(t_gpu[sid, :3], t_ref, rtol=5e-3, atol=5e-3 * max(np.linalg.norm(t_ref), 1e-3))
 
 
+@pytest.mark.parametrize("kind", ["dynamic_sphere", "effmass_sphere"])
+def test_deterministic_coupling_matches_atomic_coupling_and_oracle(kind):
+    """CRB200_OPT_DETERMINISTIC_COUPLING sums the coupling momentum per grid block in a fixed order
+    and then over blocks in ascending order: the totals must match the float-atomic totals (same
+    terms, other order: within 1e-3 relative after 100 substeps of one run each, whose grids differ
+    only by the P2G atomics' rounding) and the oracle within the bar of test_dynamic_coupling_force."""
+    sc = scenes.contact_scene(kind)
+    runs = {}
+    for det in (0, 1):
+        g = cb.DeviceScene(sc)
+        g.solver.set_option(cb.OPT_DETERMINISTIC_COUPLING, det)
+        g.step(100)
+        runs[det] = g.coupling()
+    sid = int(sc.shapes.shape_ids[0])
+    (fa, ta), (fd, td) = runs[0], runs[1]
+    assert np.linalg.norm(fa[sid, :3]) > 0.1
+    np.testing.assert_allclose(fd[sid, :3], fa[sid, :3], rtol=1e-3, atol=1e-3 * np.linalg.norm(fa[sid, :3]))
+    np.testing.assert_allclose(td[sid, :3], ta[sid, :3], rtol=1e-3, atol=1e-3 * max(np.linalg.norm(ta[sid, :3]), 1e-3))
+    r = _ref(sc)
+    r.compute_initial_data()
+    r.step(100)
+    if isinstance(r, op.RefOracle):
+        f_ref, t_ref = r.coupling()
+        f_ref, t_ref = f_ref[sid, :3], t_ref[sid, :3]
+    else:
+        c6 = r.coupling(sid)
+        f_ref, t_ref = c6[:3], c6[3:]
+    np.testing.assert_allclose(fd[sid, :3], f_ref, rtol=2e-3, atol=2e-3 * np.linalg.norm(f_ref))
+    np.testing.assert_allclose(td[sid, :3], t_ref, rtol=5e-3, atol=5e-3 * max(np.linalg.norm(t_ref), 1e-3))
+
+
+def test_deterministic_coupling_refused_on_batches():
+    b = cb.DeviceBatch([scenes.contact_scene("dynamic_sphere"), scenes.contact_scene("box")])
+    with pytest.raises(cb.CrmpmError, match="batch"):
+        b.solver.set_option(cb.OPT_DETERMINISTIC_COUPLING, 1)
+
+
 def test_pb_cutting_small():
     sc = scenes.pb_cutting(size=(0.12, 0.04, 0.12), cell=0.008, bounds_min=(-0.12, -0.1, -0.12),
                            bounds_max=(0.12, 0.1, 0.12), iterations=10)
