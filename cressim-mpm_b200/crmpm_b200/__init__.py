@@ -32,6 +32,7 @@ STATUS_BLOCK_OVERFLOW = 0x2
 STATUS_OUT_OF_DOMAIN = 0x4
 OPT_PHASE_TIMING = 3
 OPT_DETERMINISTIC_COUPLING = 4
+OPT_DETERMINISTIC = 5
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 
 

@@ -541,6 +541,11 @@ extern "C"
             if (int rc = s->setDeterministicCoupling(value != 0))
                 return rc;
         }
+        else if (option == CRB200_OPT_DETERMINISTIC)
+        {
+            if (int rc = s->setDeterministic(value != 0))
+                return rc;
+        }
         else
             return bad("CrB200SolverSetOption: unknown option");
         s->configVersion++;

@@ -223,7 +223,12 @@ namespace crb200
         bool detCoupling = false;            // CRB200_OPT_DETERMINISTIC_COUPLING
         float4 *detPartials = nullptr;       // per block and dynamic slot: force, torque partial sums
         unsigned *detMask = nullptr;         // bit per block: detPartials holds sums for it
+        bool detP2G = false;                 // CRB200_OPT_DETERMINISTIC
+        float4 *detTiles = nullptr, *detTilesF = nullptr; // per block: its P2G tile (deterministic P2G)
+        unsigned long long *detFixedMass = nullptr;       // fixed-point initial node masses
         int setDeterministicCoupling(bool on);
+        int setDeterministic(bool on);
+        int detLevel(bool recomputing) const;
         cudaStream_t sideStream = nullptr; // shape gather / cut masks beside the sort chain
         cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     };

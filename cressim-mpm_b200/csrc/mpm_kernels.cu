@@ -504,6 +504,52 @@ namespace crb200
     // Absolute start of every cell of the active blocks (one warp per block, lane l scanning cells l
     // and l + 32): the block's start plus the exclusive prefix of its cell counts, which are cleared
     // for the next binning.
+    // Deterministic substeps: each cell's slots hold its particle ids in ascending order (the
+    // scatter places them in arrival order).  One 64-thread CTA per active block: the block's ids
+    // go to shared memory (coalesced), thread c insertion-sorts cell c's segment, and they go back;
+    // a block larger than the buffer sorts in place in global memory.
+    constexpr unsigned kCellOrderCap = 2048;
+    __global__ void __launch_bounds__(64) k_cellOrder(const SortHeader *__restrict__ hdr,
+                                                      const unsigned *__restrict__ activeList,
+                                                      const unsigned *__restrict__ blockStart,
+                                                      const unsigned *__restrict__ cellStart,
+                                                      unsigned *__restrict__ sortedIds)
+    {
+        __shared__ unsigned sIds[kCellOrderCap];
+        const unsigned tid = threadIdx.x, nAct = hdr->numActiveBlocks;
+        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
+        {
+            const unsigned b = activeList[ab], start = blockStart[b], cnt = blockStart[b + 1] - start;
+            const unsigned s = cellStart[b * 64u + tid] - start;
+            const unsigned e = (tid < 63u ? cellStart[b * 64u + tid + 1u] : blockStart[b + 1]) - start;
+            unsigned *ids = cnt <= kCellOrderCap ? sIds : sortedIds + start;
+            if (cnt <= kCellOrderCap)
+            {
+                for (unsigned t = tid; t < cnt; t += 64u)
+                    sIds[t] = sortedIds[start + t];
+                __syncthreads();
+            }
+            for (unsigned i = s + 1; i < e; ++i)
+            {
+                const unsigned v = ids[i];
+                unsigned j = i;
+                while (j > s && ids[j - 1] > v)
+                {
+                    ids[j] = ids[j - 1];
+                    --j;
+                }
+                ids[j] = v;
+            }
+            if (cnt <= kCellOrderCap)
+            {
+                __syncthreads();
+                for (unsigned t = tid; t < cnt; t += 64u)
+                    sortedIds[start + t] = sIds[t];
+                __syncthreads();
+            }
+        }
+    }
+
     __global__ void __launch_bounds__(256) k_cellStarts(const SortHeader *__restrict__ hdr,
                                                         const unsigned *__restrict__ activeList,
                                                         const unsigned *__restrict__ blockStart,
@@ -541,14 +587,57 @@ namespace crb200
 #include "p2g_cells.cuh"
 namespace crb200
 {
+    // Deterministic P2G: a node's sum over the 6x6x6 tiles of the active cell blocks that cover it
+    // (its own block and, for the first two nodes along an axis, the block below), in a fixed order
+    // of (dz, dy, dx), then `rest` (what per-particle atomics added to the node).
+    __device__ __forceinline__ float4 gatherTiles(const GridGeom &g, const float4 *__restrict__ tiles,
+                                                  const unsigned char *__restrict__ flags, int bx, int by, int bz,
+                                                  unsigned l, float4 rest)
+    {
+        const int lx = l & 3, ly = (l >> 2) & 3, lz = l >> 4;
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int dz = 0; dz < 2; ++dz)
+        {
+            if (dz && (lz >= 2 || bz == 0))
+                continue;
+            for (int dy = 0; dy < 2; ++dy)
+            {
+                if (dy && (ly >= 2 || by == 0))
+                    continue;
+                for (int dx = 0; dx < 2; ++dx)
+                {
+                    if (dx && (lx >= 2 || bx == 0))
+                        continue;
+                    const unsigned c = g.blockBase + (unsigned)(bx - dx) + g.nb.x * ((unsigned)(by - dy) + g.nb.y * (unsigned)(bz - dz));
+                    if (!(flags[c] & 1u))
+                        continue;
+                    const int t = (lx + 4 * dx) + kTileEdge * ((ly + 4 * dy) + kTileEdge * (lz + 4 * dz));
+                    const float4 v = tiles[(size_t)c * kTileNodes + t];
+                    s.x += v.x;
+                    s.y += v.y;
+                    s.z += v.z;
+                    s.w += v.w;
+                }
+            }
+        }
+        s.x += rest.x;
+        s.y += rest.y;
+        s.z += rest.z;
+        s.w += rest.w;
+        return s;
+    }
+
     // 7. Grid update over touched blocks (mls_mpm_algorithm.h:243-294 and its PB / standard twins).
     //    Multi: the touched blocks belong to many scenes; each block reads its scene's parameters
     //    and shapes from global memory (single scene: kernel arguments and shared memory).
-    //    Det: coupling momentum of the first kDetSlots dynamic shapes is summed per 4x4x4 block in a
-    //    fixed order and written to detPartials[(block * kDetSlots + slot) * 2 + {0: force, 1: torque}]
-    //    (bit `block` of detMask set) for k_coupleReduce, instead of float atomics into the shapes'
-    //    force and torque.
-    template <bool Multi, bool Det>
+    //    Det >= 1: coupling momentum of the first kDetSlots dynamic shapes is summed per 4x4x4 block
+    //    in a fixed order and written to detPartials[(block * kDetSlots + slot) * 2 + {0: force,
+    //    1: torque}] (bit `block` of detMask set) for k_coupleReduce, instead of float atomics into
+    //    the shapes' force and torque.
+    //    Det == 2: the P2G grid comes from the cell blocks' tiles (k_accumulate<.., true>): each
+    //    node sums the tiles that cover it in a fixed order (gatherTiles), then what per-particle
+    //    atomics left in gridA (particles whose stencil leaves the grid).
+    template <bool Multi, int Det>
     __global__ void __launch_bounds__(256) k_gridUpdate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                         const unsigned *__restrict__ touchedList,
                                                         const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -557,7 +646,9 @@ namespace crb200
                                                         float4 *coupleTorque, bool clearA,
                                                         unsigned long long *__restrict__ blockShapeMask,
                                                         float4 *__restrict__ saveA, float4 *__restrict__ saveV,
-                                                        float4 *__restrict__ detPartials, unsigned *__restrict__ detMask)
+                                                        float4 *__restrict__ detPartials, unsigned *__restrict__ detMask,
+                                                        const float4 *__restrict__ tiles, const float4 *__restrict__ tilesF,
+                                                        const unsigned char *__restrict__ blockFlags)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
@@ -570,15 +661,15 @@ namespace crb200
         const unsigned nT = hdr->numTouchedBlocks;
         const bool withForce = p0.solverType == CRB200_SOLVER_GPU_STANDARD;
         const unsigned perCta = blockDim.x / 64;
-        using Couple = typename std::conditional<Det, CoupleRow, CoupleAtomic>::type;
-        if constexpr (Det)
+        using Couple = typename std::conditional<(Det > 0), CoupleRow, CoupleAtomic>::type;
+        if constexpr (Det > 0)
             for (int c = 0; c < kDetSlots * 6; ++c)
                 sCouple[threadIdx.x][c] = 0.f;
         for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
         {
             const unsigned bi = base + threadIdx.x / 64;
             Couple couple;
-            if constexpr (Det)
+            if constexpr (Det > 0)
                 couple = CoupleRow{sCouple[threadIdx.x], CoupleAtomic{coupleForce, coupleTorque}, false};
             else
                 couple = CoupleAtomic{coupleForce, coupleTorque};
@@ -616,6 +707,8 @@ namespace crb200
                 float4 acc = gridA[a];
                 if (clearA)
                     gridA[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (Det == 2)
+                    acc = gatherTiles(g, tiles, blockFlags, bx, by, bz, l, acc);
                 if (saveA)
                     saveA[a] = acc; // the adjoint's tape of this substep's P2G grid
                 float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -623,6 +716,8 @@ namespace crb200
                 {
                     f = gridF[a];
                     gridF[a] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (Det == 2)
+                        f = gatherTiles(g, tilesF, blockFlags, bx, by, bz, l, f);
                 }
                 {
                     // nodes that received mass (roofline bookkeeping): a shared counter per CTA
@@ -660,7 +755,7 @@ namespace crb200
                 if (saveV)
                     saveV[a] = make_float4(v.x, v.y, v.z, acc.w);
             } while (false);
-            if constexpr (Det)
+            if constexpr (Det > 0)
             {
                 // block sums in a fixed order: thread c < 24 of each 64-thread group adds column c
                 // of the group's rows in row order, writes it and clears the column
@@ -1199,6 +1294,66 @@ namespace crb200
                 }
     }
 
+    // Deterministic initial data: k_initMass's node masses as 64-bit fixed-point sums, which are
+    // exact and so independent of the order of the atomics.  The unit is (largest particle mass) /
+    // 2^50: a node sums at most a few thousand contributions of at most that mass, far below 2^63.
+    __global__ void k_initMaxMass(unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+                                  unsigned *__restrict__ maxBits)
+    {
+        const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ii >= n)
+            return;
+        const float m = xm[idx[ii]].w;
+        if (m > 0.f)
+            atomicMax(maxBits, __float_as_uint(m)); // positive floats order like their bits
+    }
+
+    __global__ void k_initMassFixed(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
+                                    float *__restrict__ F, unsigned stride, const unsigned *__restrict__ maxBits,
+                                    unsigned long long *__restrict__ fixedMass)
+    {
+        const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
+        if (ii >= n)
+            return;
+        const unsigned p = idx[ii];
+        M3 I;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            I.m[e] = (e % 4) == 0 ? 1.f : 0.f;
+        storeM3(F, stride, p, I);
+        const float4 x4 = xm[p];
+        const Stencil st = stencilOf(g, v3(x4));
+        if (!st.finite || *maxBits == 0u)
+            return;
+        const double scale = 1125899906842624.0 / (double)__uint_as_float(*maxBits); // 2^50 / max mass
+        float w[3][3];
+        weights(st.fx, w);
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c)
+                {
+                    const int ni = st.b[0] + a, nj = st.b[1] + b, nk = st.b[2] + c;
+                    if (!inGrid(g, ni, nj, nk))
+                        continue;
+                    const float q = (w[a][0] * w[b][1] * w[c][2]) * x4.w;
+                    atomicAdd(&fixedMass[nodeAddr(g, ni, nj, nk)], (unsigned long long)llrint((double)q * scale));
+                }
+    }
+
+    __global__ void k_initMassFlush(unsigned numNodes, const unsigned *__restrict__ maxBits,
+                                    unsigned long long *__restrict__ fixedMass, float4 *__restrict__ gridA)
+    {
+        const unsigned a = blockIdx.x * blockDim.x + threadIdx.x;
+        if (a >= numNodes)
+            return;
+        const unsigned long long v = fixedMass[a];
+        if (!v)
+            return;
+        fixedMass[a] = 0ull;
+        const double unit = (double)__uint_as_float(*maxBits) / 1125899906842624.0;
+        gridA[a].w += (float)((double)(long long)v * unit);
+    }
+
     __global__ void k_initVolume(GridGeom g0, SceneTable sc, unsigned n, const unsigned *__restrict__ idx,
                                  const float4 *__restrict__ xm, const float4 *__restrict__ gridA, float *__restrict__ V0)
     {
@@ -1534,7 +1689,8 @@ namespace crb200
                 cudaEventDestroy(e);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, cellCount, blockCount, blockStart,
                         activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, cellStart,
-                        dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask};
+                        dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask,
+                        detTiles, detTilesF, detFixedMass};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -1554,6 +1710,43 @@ namespace crb200
             cudaEventDestroy(joinEvent);
         if (sideStream)
             cudaStreamDestroy(sideStream);
+    }
+
+    // 0: atomics; 1: coupling reduced in a fixed order; 2: also the P2G grid from block tiles.
+    // Recomputed substeps of the adjoint keep the atomics (their coupling goes to scratch).
+    int Solver::detLevel(bool recomputing) const
+    {
+        if (isBatch() || recomputing || tapeActive >= 0 || !detPartials)
+            return 0;
+        if (detP2G && detTiles)
+            return 2;
+        return detCoupling ? 1 : 0;
+    }
+
+    // Deterministic substeps: tiles of every grid block (216 float4; twice for the standard
+    // solver's force pass), written whole by the accumulation of each active block.
+    int Solver::setDeterministic(bool on)
+    {
+        if (on && isBatch())
+        {
+            setLastError("deterministic substeps: not available on batch solvers");
+            return CRB200_ERR_UNSUPPORTED;
+        }
+        if (int rc = setDeterministicCoupling(on))
+            return rc;
+        if (on && !detTiles)
+        {
+            const size_t bytes = (size_t)totalBlocks * kTileNodes * sizeof(float4);
+            CRB_CHECK(cudaMalloc(&detTiles, bytes));
+            if (solverType == CRB200_SOLVER_GPU_STANDARD)
+                CRB_CHECK(cudaMalloc(&detTilesF, bytes));
+            // fixed-point node masses of the initial data, plus one word for the largest particle mass
+            const size_t fbytes = ((size_t)totalBlocks * 64u + 1u) * sizeof(unsigned long long);
+            CRB_CHECK(cudaMalloc(&detFixedMass, fbytes));
+            CRB_CHECK(cudaMemset(detFixedMass, 0, fbytes));
+        }
+        detP2G = on;
+        return CRB200_OK;
     }
 
     // Deterministic coupling: the block partial buffer (zeroed; the reduction keeps it zeroed).
@@ -1777,6 +1970,11 @@ namespace crb200
         int r = sortParticles(p, isStd);
         if (r != CRB200_OK)
             return r;
+        if (!Multi && nPart > 0 && detLevel(recompute || adjReplay) == 2)
+        {
+            k_cellOrder<<<cellCtas * 4, 64, 0, stream>>>(header, activeList, blockStart, cellStart, sortedIds);
+            CRB_LAUNCHED(1);
+        }
         if (fork)
             CRB_CHECK(cudaStreamWaitEvent(stream, joinEvent, 0));
         markPhase(1);
@@ -1787,32 +1985,46 @@ namespace crb200
             k_record<M, Multi><<<std::min(pg, (unsigned)strideCtas), 128, 0, stream>>>(p, sc, header, sortedIds, positionMass, velocity, matParams, matType,
                                                         F, Cm, V0, stride, cutMasks, records, gridA, gridF,
                                                         &header->fp64Fallbacks);
-            k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds, cellStart,
-                                                                records, cutMasks, gridA, gridF);
+            bool tiled = false;
+            if constexpr (!Multi)
+                if (detLevel(recompute || adjReplay) == 2)
+                {
+                    k_accumulate<M, false, true><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart,
+                                                                           sortedIds, cellStart, records, cutMasks,
+                                                                           gridA, gridF, detTiles, detTilesF);
+                    tiled = true;
+                }
+            if (!tiled)
+                k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds,
+                                                                    cellStart, records, cutMasks, gridA, gridF);
             CRB_LAUNCHED(2);
             return CRB200_OK;
         };
         auto update = [&]() -> int {
-            const bool det = detCoupling && !Multi && !(recompute || adjReplay) && detPartials != nullptr;
+            const int det = detLevel(recompute || adjReplay);
             auto upd = [&](auto detTag) {
-                constexpr bool D = decltype(detTag)::value;
+                constexpr int D = decltype(detTag)::value;
                 k_gridUpdate<Multi, D><<<updCtas, 256, 0, stream>>>(
                     p, sc, header, touchedList, shapeTable, sp, gridA, gridF, gridV, (recompute || adjReplay) ? adjForce : cf,
                     (recompute || adjReplay) ? adjTorque : ct, !recompute || tapeActive >= 0, blockShapeMask,
                     tapeActive >= 0 ? tapeSlot(tapeActive).gridA : nullptr,
                     tapeActive >= 0 ? tapeSlot(tapeActive).gridV : nullptr, D ? detPartials : nullptr,
-                    D ? detMask : nullptr);
+                    D ? detMask : nullptr, D == 2 ? detTiles : nullptr, D == 2 ? detTilesF : nullptr, blockFlags);
             };
-            if (det)
+            if constexpr (!Multi)
+                if (det != 0)
+                {
+                    if (det == 2)
+                        upd(std::integral_constant<int, 2>{});
+                    else
+                        upd(std::integral_constant<int, 1>{});
+                    k_coupleReduce<<<1, 256, 0, stream>>>((totalBlocks + 31) / 32, detMask, detPartials, shapeTable,
+                                                          numShapes, cf, ct);
+                    CRB_LAUNCHED(2);
+                }
+            if (Multi || det == 0)
             {
-                upd(std::true_type{});
-                k_coupleReduce<<<1, 256, 0, stream>>>((totalBlocks + 31) / 32, detMask, detPartials, shapeTable, numShapes,
-                                                      cf, ct);
-                CRB_LAUNCHED(2);
-            }
-            else
-            {
-                upd(std::false_type{});
+                upd(std::integral_constant<int, 0>{});
                 CRB_LAUNCHED(1);
             }
             if (tapeActive >= 0)
@@ -2089,10 +2301,25 @@ namespace crb200
         }
         const unsigned g = (n + 127) / 128;
         const SceneTable sc = sceneTable();
-        k_initMass<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, F, (unsigned)numMaxParticles, gridA);
+        if (detP2G && detFixedMass && !isBatch())
+        {
+            unsigned *maxBits = reinterpret_cast<unsigned *>(detFixedMass + (size_t)totalBlocks * 64u);
+            CRB_CHECK(cudaMemsetAsync(maxBits, 0, sizeof(unsigned), stream));
+            k_initMaxMass<<<g, 128, 0, stream>>>(n, indices, positionMass, maxBits);
+            k_initMassFixed<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, F, (unsigned)numMaxParticles, maxBits,
+                                                   detFixedMass);
+            const unsigned nodes = totalBlocks * 64u;
+            k_initMassFlush<<<(nodes + 255) / 256, 256, 0, stream>>>(nodes, maxBits, detFixedMass, gridA);
+            CRB_LAUNCHED(3);
+        }
+        else
+        {
+            k_initMass<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, F, (unsigned)numMaxParticles, gridA);
+            CRB_LAUNCHED(1);
+        }
         k_initVolume<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA, V0);
         k_initClear<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, gridA);
-        CRB_LAUNCHED(3);
+        CRB_LAUNCHED(2);
         return CRB200_OK;
     }
 

@@ -326,7 +326,11 @@ namespace crb200
 
     // (c) Cell accumulation: one 64-thread CTA per active block, one thread per cell.
     //     Multi: each active block reads its scene's parameters (block base search).
-    template <int Mode, bool Multi>
+    //     Det: nothing is added atomically.  A cell thread accumulates all of its cell's particles
+    //     (no kCellRun cap) and the block's whole 6x6x6 tile is stored to tiles[block] (tilesF for
+    //     the standard solver's force pass), from which the grid update sums each node's sources in
+    //     a fixed order.
+    template <int Mode, bool Multi, bool Det = false>
     __global__ void __launch_bounds__(64, Multi ? 5 : 6) k_accumulate(const __grid_constant__ StepParams p0, SceneTable sc, const SortHeader *__restrict__ hdr,
                                                        const unsigned *__restrict__ activeList,
                                                        const unsigned *__restrict__ blockStart,
@@ -334,7 +338,8 @@ namespace crb200
                                                        const unsigned *__restrict__ cellStart,
                                                        const float4 *__restrict__ records,
                                                        const unsigned *__restrict__ cutMasks, float4 *__restrict__ gridA,
-                                                       float4 *__restrict__ gridF)
+                                                       float4 *__restrict__ gridF, float4 *__restrict__ tiles = nullptr,
+                                                       float4 *__restrict__ tilesF = nullptr)
     {
         __shared__ unsigned sStart[65];
         __shared__ unsigned sOv[65];
@@ -394,7 +399,8 @@ namespace crb200
             }
             __syncthreads();
             const unsigned cs = sStart[tid], ce = sStart[tid + 1];
-            const unsigned runEnd = min(ce, cs + (unsigned)kCellRun);
+            // Det: a cell thread takes all of its cell's particles, so nothing goes through atomics
+            const unsigned runEnd = Det ? ce : min(ce, cs + (unsigned)kCellRun);
             for (int pass = 0; pass < passes; ++pass)
             {
                 float acc[27][4];
@@ -466,6 +472,12 @@ namespace crb200
                         sTile[0][c * kTileNodes + t] = 0.f;
                         sTile[1][c * kTileNodes + t] = 0.f;
                     }
+                    if (Det)
+                    {
+                        float4 *dst = (Mode == 2 && pass == 1) ? tilesF : tiles;
+                        dst[(size_t)b * kTileNodes + t] = make_float4(px, py, pz, m);
+                        continue;
+                    }
                     const int tx = t % kTileEdge, ty = (t / kTileEdge) % kTileEdge, tz = t / (kTileEdge * kTileEdge);
                     const int i = 4 * bx + tx, j = 4 * by + ty, k = 4 * bz + tz;
                     if (!inGrid(g, i, j, k))
@@ -480,7 +492,7 @@ namespace crb200
                         atomicAdd(&gridA[a], make_float4(px, py, pz, m));
                 }
                 // particles beyond the first kCellRun of a cell: one per thread, vector atomics
-                const unsigned total = sOv[64];
+                const unsigned total = Det ? 0u : sOv[64];
                 for (unsigned kk = tid; kk < total; kk += 64)
                 {
                     int lo = 0, hi = 63;

@@ -273,6 +273,13 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * batch).  The first switch-on allocates 128 bytes per grid block. */
 #define CRB200_OPT_PHASE_TIMING 3
 #define CRB200_OPT_DETERMINISTIC_COUPLING 4
+/* CRB200_OPT_DETERMINISTIC: substeps reproducible bit for bit from the same state.  On top of the
+ * deterministic coupling, P2G adds nothing atomically: each 4x4x4 cell block stores its whole 6x6x6
+ * node tile (3.4 KB per grid block, allocated at the first switch-on) and the grid update sums the
+ * tiles covering a node in a fixed order (the reference sums with float atomics in arrival order,
+ * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
+ * Single-scene solvers only; the adjoint's recomputed substeps use the ordinary path. */
+#define CRB200_OPT_DETERMINISTIC 5
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the

@@ -1,0 +1,77 @@
+"""Deterministic substeps (CRB200_OPT_DETERMINISTIC): P2G stores whole block tiles and the grid
+update sums each node's tiles in a fixed order; the coupling momentum is reduced in a fixed order.
+Two runs from the same state must agree bit for bit (the ordinary path sums with float atomics in
+arrival order, as the reference does, and does not), and a deterministic run must stay within the
+parity tolerance of the ordinary run and of the FP64 oracle."""
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from gpu_helpers import rel_pos_err
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
+
+import crmpm_b200 as cb  # noqa: E402
+import oracle_py as op  # noqa: E402
+from crmpm_b200 import scenes  # noqa: E402
+
+
+def _pb_cut():
+    sc = scenes.pb_cutting(size=(0.12, 0.04, 0.12), cell=0.008, bounds_min=(-0.12, -0.1, -0.12),
+                           bounds_max=(0.12, 0.1, 0.12), iterations=10)
+    sc.shapes.position[1, :3] = (0.0, -0.01, 0.0)
+    return sc
+
+
+CASES = {
+    "mls_cube": (lambda: scenes.cube_drop(), 200),
+    # 27 particles per cell: every cell overflows the 9 a cell thread accumulates
+    "mls_dense": (lambda: scenes.cube_drop(ppc=27, side=0.3), 100),
+    "dynamic_sphere": (lambda: scenes.contact_scene("dynamic_sphere"), 100),
+    "effmass_sphere": (lambda: scenes.contact_scene("effmass_sphere"), 100),
+    "pb_cutting": (_pb_cut, 5),
+    "standard_cube": (lambda: scenes.cube_drop(solver=scenes.SOLVER_STANDARD, dt=1e-4), 200),
+}
+
+
+def _run(sc, steps, det):
+    # the option goes on before the initial data: their node masses are summed deterministically too
+    g = cb.DeviceScene(sc, compute_initial=False)
+    if det:
+        g.solver.set_option(cb.OPT_DETERMINISTIC, 1)
+    g.compute_initial_data()
+    g.step(steps)
+    st = g.state()
+    f, t = g.coupling()
+    return st, f, t
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_deterministic_runs_repeat_bit_for_bit(case):
+    make, steps = CASES[case]
+    sc = make()
+    a, fa, ta = _run(sc, steps, True)
+    b, fb, tb = _run(sc, steps, True)
+    for k in ("x", "v", "F", "C"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=f"{case}: {k} differs between two deterministic runs")
+    np.testing.assert_array_equal(fa, fb)
+    np.testing.assert_array_equal(ta, tb)
+    # the ordinary (atomic) path: same physics within the parity tolerance
+    c, fc, tc = _run(sc, steps, False)
+    tol = 2e-3 if case == "pb_cutting" else 1e-4  # PB-MPM cutting amplifies rounding (see test_gpu_batch)
+    assert rel_pos_err(a["x"], c["x"], sc.pos_mass[:, :3], sc.cell_size) <= tol
+
+
+def test_deterministic_mls_cube_matches_fp64_oracle():
+    sc = scenes.cube_drop()
+    a, _, _ = _run(sc, 200, True)
+    o = op.PortOracle(sc, 64)
+    o.compute_initial_data()
+    o.step(200)
+    assert rel_pos_err(a["x"], o.state()["x"], sc.pos_mass[:, :3], sc.cell_size) <= 1e-4
+
+
+def test_deterministic_refused_on_batches():
+    b = cb.DeviceBatch(scenes.batched_scenes(num_scenes=2, nmin=1000, nmax=2000))
+    with pytest.raises(cb.CrmpmError, match="batch"):
+        b.solver.set_option(cb.OPT_DETERMINISTIC, 1)
