@@ -156,7 +156,7 @@ namespace crb200
     // written as a P2G record (base g_v, matrix 4/dx g_C^T, no mass) that k_accumulate sums into
     // gridG in cell order; stencils outside the grid are added here with atomics.
     template <bool Multi>
-    __global__ void __launch_bounds__(128, 3) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
+    __global__ void __launch_bounds__(128, 4) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
                                                    const float4 *__restrict__ xm, const unsigned char *__restrict__ mask,
                                                    const float *__restrict__ F, unsigned stride,
                                                    const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -511,7 +511,7 @@ namespace crb200
     // Reverse of P2G and of the stress (per particle); completes the adjoint of the substep's input
     // state and accumulates dL/dlambda, dL/dmu.
     template <bool Multi>
-    __global__ void __launch_bounds__(128) k_adjP2G(const __grid_constant__ StepParams p0, SceneTable sc,
+    __global__ void __launch_bounds__(128, 5) k_adjP2G(const __grid_constant__ StepParams p0, SceneTable sc,
                                                    const float4 *__restrict__ xm, const float4 *__restrict__ vel,
                                                    const unsigned char *__restrict__ mask,
                                                    const float4 *__restrict__ matParams, const float *__restrict__ F,
