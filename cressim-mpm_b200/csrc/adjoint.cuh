@@ -687,10 +687,12 @@ namespace crb200
                                 unsigned *__restrict__ blockCount, unsigned numBlockCounts,
                                 unsigned *__restrict__ cellCount, unsigned numCellCounts, unsigned *__restrict__ flag)
     {
+        // the blob has the live arrays' layout (x, v, then the F and C planes, `stride` apart), so
+        // the reverse kernels can read a saved state in place
         float4 *bx = reinterpret_cast<float4 *>(blob);
-        float4 *bv = bx + n;
-        float *bF = reinterpret_cast<float *>(bv + n);
-        float *bC = bF + 9ull * n;
+        float4 *bv = bx + stride;
+        float *bF = reinterpret_cast<float *>(bv + stride);
+        float *bC = bF + 9ull * stride;
         const unsigned stepN = gridDim.x * blockDim.x, t0 = blockIdx.x * blockDim.x + threadIdx.x;
         // x and v (float4 items), then the 18 planes of F and C (float items): independent
         // elements, so every thread has loads in flight
@@ -708,7 +710,7 @@ namespace crb200
         for (int plane = 0; plane < 18; ++plane)
         {
             float *a = plane < 9 ? F + (size_t)plane * stride : C + (size_t)(plane - 9) * stride;
-            float *b = plane < 9 ? bF + (size_t)plane * n : bC + (size_t)(plane - 9) * n;
+            float *b = plane < 9 ? bF + (size_t)plane * stride : bC + (size_t)(plane - 9) * stride;
             for (unsigned i = t0; i < n; i += stepN)
             {
                 if (load)
@@ -910,9 +912,13 @@ namespace crb200
     // One reverse substep from the tape of slot k (the replayed forward of the same input state
     // wrote its P2G grid, grid velocities and sort there); the input state itself is loaded.
     template <bool Multi>
-    int Solver::adjointSubstepTape(int k)
+    int Solver::adjointSubstepTape(int k, const unsigned char *state)
     {
         const TapeSlot ts = tapeSlot(k);
+        // the substep's input state, saved by its replay in the layout of the live arrays
+        const size_t nm = (size_t)numMaxParticles;
+        const float4 *sx = reinterpret_cast<const float4 *>(state), *sv = sx + nm;
+        const float *sF = reinterpret_cast<const float *>(sv + nm), *sC = sF + 9 * nm;
         const StepParams p = params();
         const SceneTable sc = sceneTable();
         const unsigned pg = (sc.numParticles + 127) / 128;
@@ -920,13 +926,13 @@ namespace crb200
                          reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
         const unsigned stride = (unsigned)numMaxParticles;
         CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
-        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, activeMask, F, stride, shapeTable, sp, ts.gridV, aX,
-                                                aV, aF, aC, gridG, records);
+        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, sx, activeMask, sF, stride, shapeTable, sp, ts.gridV, aX, aV, aF,
+                                                aC, gridG, records);
         k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, ts.hdr, ts.activeList, ts.blockStart, ts.sortedIds,
                                                             ts.cellStart, records, cutMasks, gridG, gridF);
         k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, ts.hdr, ts.touchedList, shapeTable, sp, ts.gridA, gridG);
-        k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, matParams, F, Cm, V0, stride,
-                                                gridG, aX, aV, aF, aC, aMat);
+        k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, sx, sv, activeMask, matParams, sF, sC, V0, stride, gridG, aX, aV,
+                                                aF, aC, aMat);
         CRB_LAUNCHED(4);
         return CRB200_OK;
     }
@@ -999,7 +1005,7 @@ namespace crb200
     }
 
     // One CUDA graph per segment slot k: replay[k] = save the state into slot k and run one forward
-    // substep, reverse[k] = load slot k and run one reverse substep.  Built once per configuration
+    // substep, reverse[k] = one reverse substep on slot k's saved state.  Built once per configuration
     // (pointers, parameters, K) and replayed for every segment of every backward pass.
     int Solver::captureGraph(int which, int k, cudaGraphExec_t *out, int *kernels)
     {
@@ -1040,12 +1046,11 @@ namespace crb200
         return r;
     }
 
+    // reverse slot k: the reverse kernels read the slot's saved input state in place
     int Solver::reverseBody(int k, size_t sb)
     {
-        int r = loadState(adjSeg + (size_t)k * sb);
-        if (r != CRB200_OK)
-            return r;
-        return isBatch() ? adjointSubstepTape<true>(k) : adjointSubstepTape<false>(k);
+        const unsigned char *slot = adjSeg + (size_t)k * sb;
+        return isBatch() ? adjointSubstepTape<true>(k, slot) : adjointSubstepTape<false>(k, slot);
     }
 
     void Solver::releaseAdjointGraphs()

@@ -194,7 +194,7 @@ namespace crb200
         size_t tapeSlotBytes() const;
         TapeSlot tapeSlot(int k) const;
         template <bool Multi>
-        int adjointSubstepTape(int k);
+        int adjointSubstepTape(int k, const unsigned char *state);
         int adjGraphKernels[3] = {0, 0, 0};
         unsigned adjGraphVersion = ~0u;
         unsigned char *adjGraphSeg = nullptr, *adjGraphTape = nullptr;
@@ -206,7 +206,8 @@ namespace crb200
         int invalidateRecords();
         int loadState(const unsigned char *src);
 
-        size_t stateBytes() const { return (size_t)totalParticles() * (2 * sizeof(float4) + 18 * sizeof(float)); }
+        // one saved state (x, v, F, C) in the layout of the live arrays
+        size_t stateBytes() const { return (size_t)numMaxParticles * (2 * sizeof(float4) + 18 * sizeof(float)); }
         int adjSubsteps = 0, adjInterval = 0;
         std::vector<int> adjCaptures;
         bool adjRecorded = false;
