@@ -339,7 +339,10 @@ def run_ours(args, rank, world, local):
 
     scene, desc = make_workload(args.workload)
     n = scene.n
-    ds = cb.DeviceScene(scene, device=dev)
+    ds = cb.DeviceScene(scene, device=dev, compute_initial=not args.deterministic)
+    if args.deterministic:  # the whole run in deterministic mode (CRB200_OPT_DETERMINISTIC)
+        ds.solver.set_option(cb.OPT_DETERMINISTIC, 1)
+        ds.compute_initial_data()
     s = ds.solver
     stream = ds.stream
     # warm-up (graph capture happens on the first replay), then the launch-shape autotuner
@@ -370,7 +373,8 @@ def run_ours(args, rank, world, local):
     ms_max = max_over_ranks(ms, world)
     value = world * n * args.steps / (ms_max / 1e3)
     if args.quick:
-        return {"metric": METRICS[args.workload], "value": value, "unit": UNITS[args.workload],
+        return {"metric": METRICS[args.workload] + (" deterministic" if args.deterministic else ""), "value": value,
+                "unit": UNITS[args.workload],
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "quick": True, "gpu_launches": int(launches)}
 
@@ -467,7 +471,7 @@ def run_ours(args, rank, world, local):
                              f"serial CPU solver arithmetic built from its own headers"}
     status = s.status()
     out = {
-        "metric": METRICS[args.workload],
+        "metric": METRICS[args.workload] + (" deterministic" if args.deterministic else ""),
         "value": value,
         "unit": UNITS[args.workload],
         "n_gpus": world,
@@ -710,6 +714,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="slab", choices=["slab", "cube", "pb", "batch", "adjoint", "sdf"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="single-scene workloads: run the timed substeps with CRB200_OPT_DETERMINISTIC on")
     ap.add_argument("--quick", action="store_true",
                     help="timed region only (no phase pass, e2e or CPU baseline): for profiler launch lists")
     args = ap.parse_args()
