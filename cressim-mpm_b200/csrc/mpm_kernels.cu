@@ -595,30 +595,29 @@ namespace crb200
                                                   unsigned l, float4 rest)
     {
         const int lx = l & 3, ly = (l >> 2) & 3, lz = l >> 4;
-        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int dz = 0; dz < 2; ++dz)
+        // all loads first (source d = 4 dz + 2 dy + dx), then the sum in that order
+        float4 v[8];
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
         {
-            if (dz && (lz >= 2 || bz == 0))
+            const int dx = d & 1, dy = (d >> 1) & 1, dz = d >> 2;
+            v[d] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if ((dx && (lx >= 2 || bx == 0)) || (dy && (ly >= 2 || by == 0)) || (dz && (lz >= 2 || bz == 0)))
                 continue;
-            for (int dy = 0; dy < 2; ++dy)
-            {
-                if (dy && (ly >= 2 || by == 0))
-                    continue;
-                for (int dx = 0; dx < 2; ++dx)
-                {
-                    if (dx && (lx >= 2 || bx == 0))
-                        continue;
-                    const unsigned c = g.blockBase + (unsigned)(bx - dx) + g.nb.x * ((unsigned)(by - dy) + g.nb.y * (unsigned)(bz - dz));
-                    if (!(flags[c] & 1u))
-                        continue;
-                    const int t = (lx + 4 * dx) + kTileEdge * ((ly + 4 * dy) + kTileEdge * (lz + 4 * dz));
-                    const float4 v = tiles[(size_t)c * kTileNodes + t];
-                    s.x += v.x;
-                    s.y += v.y;
-                    s.z += v.z;
-                    s.w += v.w;
-                }
-            }
+            const unsigned c = g.blockBase + (unsigned)(bx - dx) + g.nb.x * ((unsigned)(by - dy) + g.nb.y * (unsigned)(bz - dz));
+            if (!(__ldg(&flags[c]) & 1u))
+                continue;
+            const int t = (lx + 4 * dx) + kTileEdge * ((ly + 4 * dy) + kTileEdge * (lz + 4 * dz));
+            v[d] = tiles[(size_t)c * kTileNodes + t];
+        }
+        float4 s = v[0];
+#pragma unroll
+        for (int d = 1; d < 8; ++d)
+        {
+            s.x += v[d].x;
+            s.y += v[d].y;
+            s.z += v[d].z;
+            s.w += v[d].w;
         }
         s.x += rest.x;
         s.y += rest.y;
@@ -647,6 +646,7 @@ namespace crb200
                                                         unsigned long long *__restrict__ blockShapeMask,
                                                         float4 *__restrict__ saveA, float4 *__restrict__ saveV,
                                                         float4 *__restrict__ detPartials, unsigned *__restrict__ detMask,
+                                                        unsigned detMaskWords,
                                                         const float4 *__restrict__ tiles, const float4 *__restrict__ tilesF,
                                                         const unsigned char *__restrict__ blockFlags)
     {
@@ -774,7 +774,10 @@ namespace crb200
                         float *dst = reinterpret_cast<float *>(&detPartials[((size_t)b * kDetSlots + slot) * 2 + c / 3]);
                         dst[c % 3] = t;
                         if (l == 0)
+                        {
                             atomicOr(&detMask[b >> 5], 1u << (b & 31)); // the block holds partials
+                            atomicOr(&detMask[detMaskWords], 1u);        // and so does the substep
+                        }
                     }
                     __syncthreads();
                 }
@@ -795,6 +798,12 @@ namespace crb200
                                                           float4 *force, float4 *torque)
     {
         __shared__ float sSum[256][kDetSlots * 6 + 1];
+        // word numMaskWords is set when any block holds partials (not on substeps without coupling)
+        if (detMask[numMaskWords] == 0u)
+            return;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            detMask[numMaskWords] = 0u;
         float t[kDetSlots * 6];
 #pragma unroll
         for (int c = 0; c < kDetSlots * 6; ++c)
@@ -1760,7 +1769,7 @@ namespace crb200
         if (on && !detPartials)
         {
             const size_t bytes = (size_t)totalBlocks * kDetSlots * 2 * sizeof(float4);
-            const size_t maskBytes = (size_t)(totalBlocks + 31) / 32 * sizeof(unsigned);
+            const size_t maskBytes = ((size_t)(totalBlocks + 31) / 32 + 1) * sizeof(unsigned); // + the "any" word
             CRB_CHECK(cudaMalloc(&detPartials, bytes));
             CRB_CHECK(cudaMemset(detPartials, 0, bytes));
             CRB_CHECK(cudaMalloc(&detMask, maskBytes));
@@ -2009,7 +2018,8 @@ namespace crb200
                     (recompute || adjReplay) ? adjTorque : ct, !recompute || tapeActive >= 0, blockShapeMask,
                     tapeActive >= 0 ? tapeSlot(tapeActive).gridA : nullptr,
                     tapeActive >= 0 ? tapeSlot(tapeActive).gridV : nullptr, D ? detPartials : nullptr,
-                    D ? detMask : nullptr, D == 2 ? detTiles : nullptr, D == 2 ? detTilesF : nullptr, blockFlags);
+                    D ? detMask : nullptr, (totalBlocks + 31) / 32, D == 2 ? detTiles : nullptr, D == 2 ? detTilesF : nullptr,
+                    blockFlags);
             };
             if constexpr (!Multi)
                 if (det != 0)
