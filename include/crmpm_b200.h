@@ -278,7 +278,7 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * node tile (3.4 KB per grid block, allocated at the first switch-on) and the grid update sums the
  * tiles covering a node in a fixed order (the reference sums with float atomics in arrival order,
  * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
- * Single-scene solvers only; the adjoint's recomputed substeps use the ordinary path. */
+ * Single-scene solvers only; the substeps an adjoint backward pass replays use the ordinary path. */
 #define CRB200_OPT_DETERMINISTIC 5
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
