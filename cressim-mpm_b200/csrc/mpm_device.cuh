@@ -800,9 +800,26 @@ namespace crb200
                 if (apq == T(0))
                     continue;
                 const T app = S[p], aqq = S[q];
-                const T theta = (aqq - app) / (T(2) * apq);
-                const T t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
-                const T c = T(1) / sqrt(t * t + T(1)), sn = t * c;
+                T theta, t, c;
+                if constexpr (sizeof(T) == 4)
+                {
+                    // single precision: hardware reciprocal, reciprocal square root and approximate
+                    // division; the sweeps converge all the same and the ill-conditioned cases are
+                    // redone in double precision
+                    theta = __fdividef(aqq - app, 2.f * apq);
+                    const float h = theta * theta + 1.f;
+                    // |theta| beyond 1e18: theta^2 overflows; t -> 1 / (2 theta)
+                    t = fabsf(theta) > 1e18f ? 0.5f / theta
+                                             : __fdividef(theta >= 0.f ? 1.f : -1.f, fabsf(theta) + h * rsqrtf(h));
+                    c = rsqrtf(t * t + 1.f);
+                }
+                else
+                {
+                    theta = (aqq - app) / (T(2) * apq);
+                    t = (theta >= T(0) ? T(1) : T(-1)) / (fabs(theta) + sqrt(theta * theta + T(1)));
+                    c = T(1) / sqrt(t * t + T(1));
+                }
+                const T sn = t * c;
                 // rotate S in the (p, q) plane: new diagonal and the off-diagonals with the third index
                 const int o = 3 - p - q;
                 const int ipo = (p == 0 && o == 1) || (p == 1 && o == 0) ? 3 : ((p == 0 && o == 2) || (p == 2 && o == 0) ? 4 : 5);
