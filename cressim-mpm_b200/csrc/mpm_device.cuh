@@ -868,12 +868,22 @@ namespace crb200
         {
             const int p = gi == 2 ? 1 : 0, q = gi == 0 ? 1 : 2, col = gi == 2 ? 1 : 0;
             const T x = B[p][col], y = B[q][col];
-            const T rr = sqrt(x * x + y * y);
+            const T r2 = x * x + y * y;
             T c = T(1), sn = T(0);
-            if (rr > T(0))
+            if (r2 > T(0))
             {
-                c = x / rr;
-                sn = y / rr;
+                if constexpr (sizeof(T) == 4)
+                {
+                    const float inv = rsqrtf(r2); // r2 is a normal float here or the matrix is degenerate
+                    c = x * inv;
+                    sn = y * inv;
+                }
+                else
+                {
+                    const T rr = sqrt(r2);
+                    c = x / rr;
+                    sn = y / rr;
+                }
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k)
