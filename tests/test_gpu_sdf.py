@@ -8,6 +8,8 @@ order, bit-identical grids (distance, gradient, NaN pattern); against the refere
 tests/test_sdf_oracle.py (identical dimensions, signs and off-mesh nodes; distances within 1e-7
 and bit-identical at >= 97 % of the nodes; gradients bit-identical where the distance stencil is).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -159,3 +161,38 @@ def test_gpu_built_sdf_drives_contact_like_the_reference_built_one(slicer):
     assert e <= 1e-4, e
     moved = np.abs(exp["x"] - sc_ref.pos_mass[:, :3]).max()
     assert moved > 0.01  # the bodies did meet
+
+
+ADAPTER_CHECK = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                             "sdf_adapter_check")
+
+
+@pytest.mark.skipif(not os.path.exists(ADAPTER_CHECK), reason="oracle/_ref/sdf_adapter_check not built")
+@pytest.mark.parametrize("slicer", [False, True], ids=["trimesh", "mesh_slicer"])
+def test_reference_side_adapter_matches_reference_builder(slicer, tmp_path):
+    """The drop-in for the factory (adapter/gpu_b200_sdf_builder.h) run against the reference's
+    own SdfBuilder in one program, as createGeometry would call them: same descriptor, same off-mesh
+    nodes (up to the reference's order-dependent slicer flag), signs equal, distances within 1e-7."""
+    import subprocess
+
+    if slicer:
+        P, T = meshes.blade(0.1, 0.04, 0.01, 10, 4)
+        cell, fatten = 0.004, 0.01
+    else:
+        P, T = meshes.torus(0.25, 0.08, 24, 12)
+        cell, fatten = 0.02, 0.04
+    path = tmp_path / "mesh.bin"
+    with open(path, "wb") as f:
+        np.asarray([len(P), len(T)], np.int32).tofile(f)
+        np.ascontiguousarray(P, np.float32).tofile(f)
+        np.ascontiguousarray(T, np.uint32).tofile(f)
+    r = subprocess.run([ADAPTER_CHECK, str(path), str(cell), str(fatten), str(int(slicer))], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = dict(zip(r.stdout.split()[0::2], r.stdout.split()[1::2]))
+    nodes = int(f["nodes"])
+    assert int(f["desc_same"]) == 1
+    assert int(f["sign_differ"]) == 0
+    assert float(f["maxdiff"]) <= 1e-7
+    assert int(f["differ"]) <= 0.03 * nodes
+    assert int(f["nan_differ"]) <= 0.005 * nodes
