@@ -173,3 +173,47 @@ def test_advance_sync_and_async_match_the_oracle():
         assert rel_pos_err(hx[:, :3], ref["x"], x0, sc.cell_size) <= POS_TOL, mode
         np.testing.assert_array_equal(hx[:, 3], sc.pos_mass[:, 3])  # masses travel with positions
     np.testing.assert_allclose(out["sync"][0][:, :3], out["async"][0][:, :3], atol=1e-6)
+
+
+SOLVER_ADAPTER_CHECK = __import__("os").path.join(
+    __import__("os").path.dirname(__import__("os").path.dirname(__import__("os").path.abspath(__file__))),
+    "oracle", "_ref", "solver_adapter_check")
+
+
+@pytest.mark.skipif(not __import__("os").path.exists(SOLVER_ADAPTER_CHECK),
+                    reason="oracle/_ref/solver_adapter_check not built")
+@pytest.mark.parametrize("solver", [scenes.SOLVER_MLS, scenes.SOLVER_PB, scenes.SOLVER_STANDARD])
+def test_reference_side_solver_adapter_runs_the_engine(solver, tmp_path):
+    """The drop-in solver (adapter/gpu_b200_mpm_solver.h) driven through the reference's own
+    MpmSolverBase / MpmSolverGpu members, in the factory's and the scene's order, gives the
+    engine's result (float atomics aside) and stays within the parity tolerance of the oracle."""
+    import subprocess
+
+    dt = {scenes.SOLVER_MLS: 2e-4, scenes.SOLVER_PB: 2e-3, scenes.SOLVER_STANDARD: 1e-4}[solver]
+    sc = scenes.cube_drop(solver=solver, dt=dt)
+    if solver == scenes.SOLVER_PB:
+        sc.mat_params[:, :2] = (1.0, 0.9)
+    steps = 10 if solver == scenes.SOLVER_PB else 100
+    path, out = tmp_path / "scene.bin", tmp_path / "out.bin"
+    with open(path, "wb") as f:
+        np.asarray([sc.n, solver], np.int32).tofile(f)
+        np.asarray([sc.cell_size, sc.dt, *sc.grid_min, *sc.grid_max, *sc.gravity, 0.3, 1.0], np.float32).tofile(f)
+        for a in (sc.pos_mass, sc.vel, sc.mat_params):
+            np.ascontiguousarray(a, np.float32).tofile(f)
+        np.ascontiguousarray(sc.mat_type, np.int32).tofile(f)
+    r = subprocess.run([SOLVER_ADAPTER_CHECK, str(path), str(steps), str(out)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    res = np.fromfile(out, np.float32).reshape(2, sc.n, 4)
+    # the PB-MPM adapter keeps the reference's default of 10 solver iterations (setSolverIterations)
+    sc.iterations = 10
+    g = _gpu(sc)
+    g.step(steps)
+    a = g.state()
+    x0 = sc.pos_mass[:, :3]
+    assert rel_pos_err(res[0, :, :3], a["x"], x0, sc.cell_size) <= 1e-4
+    o = op.PortOracle(sc, 64)
+    o.compute_initial_data()
+    o.step(steps)
+    tol = 2e-3 if solver == scenes.SOLVER_PB else 1e-4
+    assert rel_pos_err(res[0, :, :3], o.state()["x"], x0, sc.cell_size) <= tol
