@@ -157,7 +157,7 @@ def barrier(world):
 METRICS = {
     "slab": "particle-substeps/s (MLS-MPM 1.6M p)",
     "cube": "particle-substeps/s (MLS-MPM 4096-particle cube)",
-    "pb": "particle-steps/s (PB-MPM cutting, 562k p, 20 iterations per step)",
+    "pb": "particle-steps/s (PB-MPM cutting, 540k p, 20 iterations per step)",
     "sdf": "SDF grid nodes/s (triangle-mesh SDF build, 5120-triangle sphere, 129^3 nodes)",
 }
 UNITS = {"slab": "particle-substeps/s", "cube": "particle-substeps/s", "pb": "particle-steps/s", "sdf": "nodes/s"}
@@ -716,13 +716,14 @@ def run_reference(args, rank, world):
     v, done, el = cpu_reference_run(scene, steps=args.steps, warmup=min(args.warmup, 3), budget_s=150.0)
     if v is None:
         return {"impl": "reference", "unavailable": "reference CPU solver driver (oracle/_ref) is not built"}
-    sample = (f"{done} of {args.steps} requested MLS substeps of the 1.6M-particle slab timed ({el:.1f} s), "
+    sample = (f"{done} of {args.steps} requested steps of the workload ({scene.n} particles) timed ({el:.1f} s), "
               f"reference serial CPU solver arithmetic built from its own headers")
-    return {
+    gpu = reference_gpu_run(scene, args)
+    line = {
         "impl": "reference",
         "metric": METRICS[args.workload],
         "value": v,
-        "unit": "particle-substeps/s",
+        "unit": UNITS[args.workload],
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -733,9 +734,34 @@ def run_reference(args, rank, world):
         "dtype": "f32",
         "data": "synthetic (seeded jittered particles)",
         "config": {"workload": desc, "particles": scene.n, "substeps_per_step": 1},
-        "cpu_baseline": {"value": v, "unit": "particle-substeps/s", "cores": 1, "kind": "reference", "sample": sample},
-        "e2e": {"value": v, "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": v, "unit": UNITS[args.workload], "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNITS[args.workload], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if gpu is not None:
+        line["reference_gpu"] = gpu
+    return line
+
+
+def reference_gpu_run(scene, args):
+    """The reference's own CUDA solver (oracle/_ref/ref_gpu_driver: src/solver/gpu_*_mpm_solver.cu
+    built for sm_100a) on the same workload, timed with CUDA events on its stream after warm-up
+    substeps, inputs resident in HBM.  None when the driver is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as op
+
+    if not op.ref_gpu_available():
+        return None
+    steps = min(args.steps, 500 if scene.solver_type != 3 else 100)
+    try:
+        r = op.ref_gpu_run(scene, steps, warmup=max(args.warmup, 3))
+    except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:
+        return {"unavailable": str(e).splitlines()[0][:200]}
+    ms = r["ms_per_substep"]
+    return {"value": scene.n / (ms / 1e3), "unit": UNITS[args.workload], "ms_per_step": ms, "steps": steps,
+            "warmup": max(args.warmup, 3),
+            "note": "the reference's GpuMlsMpmSolver / GpuPbMpmSolver / GpuStandardMpmSolver compiled from its own "
+                    "sources for sm_100a (-O3), driven through its MpmSolver interface; CUDA events around the "
+                    "timed substeps"}
 
 
 def main():

@@ -424,3 +424,71 @@ def port_sdf(points, triangles, cell: float, fatten: float = 0.0, normalize: boo
     L.oracle_sdf_build(_p(P), P.shape[0], _p(T), T.shape[0], _p(dims), _p(lower), cell, int(slicer), _p(sp),
                        int(normalize), _p(out))
     return tuple(int(v) for v in dims), lower, size, out
+
+
+# The reference's own CUDA solvers (oracle/_ref/ref_gpu_driver, built by `make -C oracle ref-gpu`
+# from src/solver/gpu_*_mpm_solver.cu): GPU-vs-GPU parity and the reference's GPU substep time.
+REF_GPU_DRIVER = os.path.join(HERE, "_ref", "ref_gpu_driver")
+_ANALYTIC_GEOMETRIES = (0, 1, 2, 3, 5, 8)  # box, sphere, plane, capsule, quad slicer, arc
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_DRIVER)
+
+
+def write_ref_gpu_scene(sc, path: str) -> None:
+    """Write a scene in the layout ref_gpu_driver.cu reads (analytic geometries only)."""
+    st = sc.shapes
+    if any(int(t) not in _ANALYTIC_GEOMETRIES for t in st.geom_type):
+        raise ValueError("ref_gpu_driver takes analytic geometries only")
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+    i32 = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+    with open(path, "wb") as f:
+        i32([sc.n, sc.solver_type, sc.iterations, sc.contact_model]).tofile(f)
+        f32([sc.cell_size, sc.dt, *sc.grid_min, *sc.grid_max, *sc.gravity]).tofile(f)
+        for a in (sc.pos_mass, sc.vel, sc.mat_params):
+            f32(a).tofile(f)
+        i32(sc.mat_type).tofile(f)
+        np.ascontiguousarray(sc.mask, np.uint8).tofile(f)
+        S = int(st.shape_type.shape[0])
+        i32([S]).tofile(f)
+        i32(st.shape_type).tofile(f)
+        i32(st.geom_idx).tofile(f)
+        for a in (st.position, st.rotation, st.inv_scale, st.lin_vel, st.ang_vel, st.com_inv_mass, st.inertia0,
+                  st.inertia1, st.params0):
+            f32(a).reshape(S, 4).tofile(f)
+        i32([st.shape_ids.shape[0]]).tofile(f)
+        i32(st.shape_ids).tofile(f)
+        i32([st.geom_type.shape[0]]).tofile(f)
+        i32(st.geom_type).tofile(f)
+        f32(st.geom_params).tofile(f)
+        i32([st.sdf_dims.shape[0]]).tofile(f)
+        i32(st.sdf_dims).tofile(f)
+        f32(st.sdf_lbcs).tofile(f)
+        i32([st.sdf_data.shape[0]]).tofile(f)
+        f32(st.sdf_data).tofile(f)
+
+
+def ref_gpu_run(sc, steps: int, warmup: int = 0, workdir: str = None, timeout: float = 600.0) -> dict:
+    """Run the reference's CUDA solver on `sc`: `warmup` substeps, then `steps` timed ones.
+
+    Returns {"x", "v" [n,3], "force", "torque" [S,4], "ms_per_substep"}; the state is after
+    warmup + steps substeps.
+    """
+    import tempfile
+
+    with tempfile.TemporaryDirectory(dir=workdir) as d:
+        scene, out = os.path.join(d, "scene.bin"), os.path.join(d, "out.bin")
+        write_ref_gpu_scene(sc, scene)
+        r = subprocess.run([REF_GPU_DRIVER, scene, str(warmup), str(steps), out], capture_output=True, text=True,
+                           timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_gpu_driver exited {r.returncode}: {r.stdout}{r.stderr}")
+        S = int(sc.shapes.shape_type.shape[0])
+        res = np.fromfile(out, np.float32)
+    n = sc.n
+    pm, vel = res[:4 * n].reshape(n, 4), res[4 * n:8 * n].reshape(n, 4)
+    ft = res[8 * n:].reshape(2, S, 4)
+    ms = float(r.stdout.split()[1])
+    return {"x": pm[:, :3].copy(), "mass": pm[:, 3].copy(), "v": vel[:, :3].copy(), "force": ft[0], "torque": ft[1],
+            "ms_per_substep": ms}
