@@ -20,6 +20,7 @@
 namespace crb200
 {
     constexpr int kAdjMaxHits = 8; // contacts per particle / node that one reverse step can undo
+    constexpr int kAdjThreads = 128; // threads per CTA of the per-particle reverse kernels
 
     // Signed distance, unit normal and the local frame quantities of shape r at world point pos,
     // exactly as rigidContact evaluates them (mpm_rigid_contact.h:129-148).
@@ -142,13 +143,6 @@ namespace crb200
         return s;
     }
 
-    __device__ __forceinline__ void loadAdj9(const float *planes, unsigned stride, unsigned i, float m[9])
-    {
-#pragma unroll
-        for (int k = 0; k < 9; ++k)
-            m[k] = planes[k * stride + i];
-    }
-
     // ---------------------------------------------------------------------------------------
     // Reverse of G2P (per particle).  In: adjoint of the substep's output state in aX, aV, aF, aC.
     // Out: aX, aF hold the G2P part of the adjoint of the input x and F.  dL/dV_n =
@@ -156,7 +150,7 @@ namespace crb200
     // written as a P2G record (base g_v, matrix 4/dx g_C^T, no mass) that k_accumulate sums into
     // gridG in cell order; stencils outside the grid are added here with atomics.
     template <bool Multi>
-    __global__ void __launch_bounds__(128, 4) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
+    __global__ void __launch_bounds__(kAdjThreads, 4) k_adjG2P(const __grid_constant__ StepParams p0, SceneTable sc,
                                                    const float4 *__restrict__ xm, const unsigned char *__restrict__ mask,
                                                    const float *__restrict__ F, unsigned stride,
                                                    const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
@@ -166,19 +160,37 @@ namespace crb200
                                                    float4 *__restrict__ records)
     {
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        // the particle's streams, staged at entry (launched with kAdjThreads threads)
+        __shared__ float4 sX[kAdjThreads], sAx[kAdjThreads], sAv[kAdjThreads];
+        __shared__ float sF[9][kAdjThreads], sAF[9][kAdjThreads], sAC[9][kAdjThreads];
+        const unsigned t = threadIdx.x;
+        const unsigned i = blockIdx.x * blockDim.x + t;
+        const bool inRange = i < (Multi ? sc.numParticles : p0.numActive);
+        if (inRange)
+        {
+            stage16(&sX[t], &xm[i]);
+            stage16(&sAx[t], &aX[i]);
+            stage16(&sAv[t], &aV[i]);
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+            {
+                stage4(&sF[k][t], &F[k * stride + i]);
+                stage4(&sAF[k][t], &aF[k * stride + i]);
+                stage4(&sAC[k][t], &aC[k * stride + i]);
+            }
+        }
         if (!Multi && p0.numShapes > 0)
             loadShapes(sh, shapeTable, p0.numShapes);
+        const bool active = inRange && mask[i] != 0;
+        const unsigned si = (Multi && inRange) ? sc.particleScene[i] : 0u;
+        stageWait();
         __syncthreads();
-        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
-            return;
-        const unsigned si = Multi ? sc.particleScene[i] : 0u;
-        if (Multi && si == 0xFFFFu)
+        if (!active || (Multi && si == 0xFFFFu))
             return;
         const StepParams &p = Multi ? sc.params[si] : p0;
         const GridGeom &g = p.g;
         const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
-        const V3 x = v3(xm[i]);
+        const V3 x = v3(sX[t]);
         const Stencil st = stencilOf(g, x);
         if (!st.finite)
             return;
@@ -187,11 +199,15 @@ namespace crb200
         weightGrads(st.fx, dw);
         // adjoint inputs; g_C' + dt g_F' F^T depends on them only, so the x-gradient moments can be
         // gathered in the same pass as the forward replay of v' and C'
-        const float4 gx4 = aX[i], gv4 = aV[i];
+        const float4 gx4 = sAx[t], gv4 = sAv[t];
         float gFo[9], gCt[9], Fp[9];
-        loadAdj9(aF, stride, i, gFo);
-        loadAdj9(aC, stride, i, gCt);
-        loadAdj9(F, stride, i, Fp);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            gFo[k] = sAF[k][t];
+            gCt[k] = sAC[k][t];
+            Fp[k] = sF[k][t];
+        }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -511,7 +527,7 @@ namespace crb200
     // Reverse of P2G and of the stress (per particle); completes the adjoint of the substep's input
     // state and accumulates dL/dlambda, dL/dmu.
     template <bool Multi>
-    __global__ void __launch_bounds__(128, 5) k_adjP2G(const __grid_constant__ StepParams p0, SceneTable sc,
+    __global__ void __launch_bounds__(kAdjThreads, 5) k_adjP2G(const __grid_constant__ StepParams p0, SceneTable sc,
                                                    const float4 *__restrict__ xm, const float4 *__restrict__ vel,
                                                    const unsigned char *__restrict__ mask,
                                                    const float4 *__restrict__ matParams, const float *__restrict__ F,
@@ -521,15 +537,34 @@ namespace crb200
                                                    float *__restrict__ aF, float *__restrict__ aC,
                                                    float4 *__restrict__ aMat)
     {
-        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
+        // the particle's streams, staged at entry (launched with kAdjThreads threads)
+        __shared__ float4 sX[kAdjThreads], sVel[kAdjThreads], sMp[kAdjThreads], sAx[kAdjThreads], sAm[kAdjThreads];
+        __shared__ float sF[9][kAdjThreads], sC[9][kAdjThreads], sAF[9][kAdjThreads], sV0[kAdjThreads];
+        const unsigned t = threadIdx.x;
+        const unsigned i = blockIdx.x * blockDim.x + t;
+        if (i >= (Multi ? sc.numParticles : p0.numActive))
             return;
+        stage16(&sX[t], &xm[i]);
+        stage16(&sVel[t], &vel[i]);
+        stage16(&sMp[t], &matParams[i]);
+        stage16(&sAx[t], &aX[i]);
+        stage16(&sAm[t], &aMat[i]);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            stage4(&sF[k][t], &F[k * stride + i]);
+            stage4(&sC[k][t], &Cm[k * stride + i]);
+            stage4(&sAF[k][t], &aF[k * stride + i]);
+        }
+        stage4(&sV0[t], &V0[i]);
+        const bool active = mask[i] != 0;
         const unsigned si = Multi ? sc.particleScene[i] : 0u;
-        if (Multi && si == 0xFFFFu)
+        stageWait();
+        if (!active || (Multi && si == 0xFFFFu))
             return;
         const StepParams &p = Multi ? sc.params[si] : p0;
         const GridGeom &g = p.g;
-        const float4 x4 = xm[i];
+        const float4 x4 = sX[t];
         const float m = x4.w;
         const Stencil st = stencilOf(g, v3(x4));
         if (!st.finite)
@@ -538,19 +573,23 @@ namespace crb200
         weights(st.fx, w);
         weightGrads(st.fx, dw);
         M3 Fp, Cp;
-        loadM3(F, stride, i, Fp);
-        loadM3(Cm, stride, i, Cp);
-        const float4 mp = matParams[i];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+        {
+            Fp.m[k] = sF[k][t];
+            Cp.m[k] = sC[k][t];
+        }
+        const float4 mp = sMp[t];
         const float lam = mp.x, mu = mp.y;
         const float J = det3(Fp);
         const float Jc = J < 1e-6f ? 1e-6f : J;
         const M3 tau = kirchhoffStress(Fp, lam, mu, 1);
-        const float coef = -p.dt * 4.f * g.invDx * g.invDx * V0[i];
+        const float coef = -p.dt * 4.f * g.invDx * g.invDx * sV0[t];
         M3 A;
 #pragma unroll
         for (int e = 0; e < 9; ++e)
             A.m[e] = tau.m[e] * coef + Cp.m[e] * m;
-        const V3 u = (v3(vel[i]) + v3(p.gravity) * p.dt) * m;
+        const V3 u = (v3(sVel[t]) + v3(p.gravity) * p.dt) * m;
         // node value u + A d_n = u' + sum_c a_c o_c with u' = u - A (fx dx), a_c = dx A(:, c)
         const V3 fd = v3(st.fx.x * g.dx, st.fx.y * g.dx, st.fx.z * g.dx);
         const V3 up = u - v3(A.m[0] * fd.x + A.m[3] * fd.y + A.m[6] * fd.z, A.m[1] * fd.x + A.m[4] * fd.y + A.m[7] * fd.z,
@@ -637,16 +676,16 @@ namespace crb200
                 for (int r = 0; r < 3; ++r)
                     gF[3 * c + r] += lam * trg * Fi.m[3 * r + c];
         }
-        const float4 ax = aX[i];
+        const float4 ax = sAx[t];
         aX[i] = make_float4(ax.x + gx.x, ax.y + gx.y, ax.z + gx.z, 0.f);
         aV[i] = make_float4(gu.x * m, gu.y * m, gu.z * m, 0.f);
 #pragma unroll
         for (int e = 0; e < 9; ++e)
         {
-            aF[e * stride + i] += gF[e];
+            aF[e * stride + i] = sAF[e][t] + gF[e];
             aC[e * stride + i] = gA[e] * m;
         }
-        const float4 am = aMat[i];
+        const float4 am = sAm[t];
         aMat[i] = make_float4(am.x + dlam, am.y + dmu, 0.f, 0.f);
     }
 
@@ -921,17 +960,17 @@ namespace crb200
         const float *sF = reinterpret_cast<const float *>(sv + nm), *sC = sF + 9 * nm;
         const StepParams p = params();
         const SceneTable sc = sceneTable();
-        const unsigned pg = (sc.numParticles + 127) / 128;
+        const unsigned pg = (sc.numParticles + kAdjThreads - 1) / kAdjThreads;
         const SdfPtrs sp{reinterpret_cast<const int4 *>(sdf.dimension), reinterpret_cast<const float4 *>(sdf.lowerBoundCellSize),
                          reinterpret_cast<const float4 *>(sdf.gradientSignedDistance)};
         const unsigned stride = (unsigned)numMaxParticles;
         CRB_CHECK(cudaMemsetAsync(gridG, 0, (size_t)totalBlocks * 64 * sizeof(float4), stream));
-        k_adjG2P<Multi><<<pg, 128, 0, stream>>>(p, sc, sx, activeMask, sF, stride, shapeTable, sp, ts.gridV, aX, aV, aF,
+        k_adjG2P<Multi><<<pg, kAdjThreads, 0, stream>>>(p, sc, sx, activeMask, sF, stride, shapeTable, sp, ts.gridV, aX, aV, aF,
                                                 aC, gridG, records);
         k_accumulate<0, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, ts.hdr, ts.activeList, ts.blockStart, ts.sortedIds,
                                                             ts.cellStart, records, cutMasks, gridG, gridF);
         k_adjGridUpdate<Multi><<<updCtas, 256, 0, stream>>>(p, sc, ts.hdr, ts.touchedList, shapeTable, sp, ts.gridA, gridG);
-        k_adjP2G<Multi><<<pg, 128, 0, stream>>>(p, sc, sx, sv, activeMask, matParams, sF, sC, V0, stride, gridG, aX, aV,
+        k_adjP2G<Multi><<<pg, kAdjThreads, 0, stream>>>(p, sc, sx, sv, activeMask, matParams, sF, sC, V0, stride, gridG, aX, aV,
                                                 aF, aC, aMat);
         CRB_LAUNCHED(4);
         return CRB200_OK;

@@ -168,6 +168,27 @@ namespace crb200
             planes[k * stride + i] = m.m[k];
     }
 
+    // Per-thread asynchronous global -> shared copies (cp.async).  A thread stages its own
+    // particle's streams, all in flight at once without holding registers, and waits for them with
+    // stageWait; no other thread reads them, so no block barrier is needed.  Every thread that
+    // issued copies waits before it exits.
+    __device__ __forceinline__ void stage4(float *dst, const float *src)
+    {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    }
+    __device__ __forceinline__ void stage16(float4 *dst, const float4 *src)
+    {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src)
+                     : "memory");
+    }
+    __device__ __forceinline__ void stageWait()
+    {
+        asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    }
+
     __device__ __forceinline__ void loadShapes(ShapeRec *dst, const ShapeRec *src, int num)
     {
         const int words = num * (int)(sizeof(ShapeRec) / sizeof(float4));

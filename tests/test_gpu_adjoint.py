@@ -83,8 +83,10 @@ def test_gpu_adjoint_matches_fp64_adjoint(kind):
 def test_gpu_adjoint_matches_central_differences():
     """Central differences of the GPU forward itself, on 120 substeps of impact with targets made at
     another material (E 3e4, nu 0.3) so that the loss depends strongly on E and nu.  Steps: 0.3 %
-    of E and nu, 1e-3 m/s for v0; the loss is summed in float64.  Tolerance 1e-3 for E, 2e-3 for
-    nu and v0 (float32 forward runs put about 1e-3 of noise into the differences themselves)."""
+    of E and nu, 1e-3 m/s for v0; the loss is summed in float64.  The float32 forward sums with
+    atomics in a varying order, so one central difference scatters by up to 1.2e-3 between runs
+    while the adjoint itself repeats to 1e-5: the E and nu differences are averaged over two
+    evaluations and held to 2e-3, v0 to 2e-3."""
     import torch
 
     steps, caps = 120, (40, 80, 120)
@@ -113,9 +115,9 @@ def test_gpu_adjoint_matches_central_differences():
     ((pos.double() - T) ** 2).mean(dim=(1, 2)).sum().backward()
     gE, gnu, gv = float(Et.grad), float(nut.grad), v0.grad.double().sum(0).cpu().numpy()
     h = 3e-3
-    fE = (L(E=E0 * (1 + h)) - L(E=E0 * (1 - h))) / (2 * E0 * h)
-    fnu = (L(nu=NU0 * (1 + h)) - L(nu=NU0 * (1 - h))) / (2 * NU0 * h)
-    assert abs(gE - fE) <= 1e-3 * abs(fE), (gE, fE)
+    fE = sum((L(E=E0 * (1 + h)) - L(E=E0 * (1 - h))) / (2 * E0 * h) for _ in range(2)) / 2
+    fnu = sum((L(nu=NU0 * (1 + h)) - L(nu=NU0 * (1 - h))) / (2 * NU0 * h) for _ in range(2)) / 2
+    assert abs(gE - fE) <= 2e-3 * abs(fE), (gE, fE)
     assert abs(gnu - fnu) <= 2e-3 * abs(fnu), (gnu, fnu)
     for k in range(3):
         dv = np.zeros(3)
