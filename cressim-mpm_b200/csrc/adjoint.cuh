@@ -1072,16 +1072,50 @@ namespace crb200
         return CRB200_OK;
     }
 
-    // replay slot k: keep the input state, run the forward substep writing slot k's tape (the
-    // segment's last slot: only up to the grid update)
+    // The state blob of segment slot k, in the layout of the live arrays.
+    Solver::StateView Solver::slotState(int k, size_t sb) const
+    {
+        const size_t nm = (size_t)numMaxParticles;
+        StateView v;
+        v.x = reinterpret_cast<float4 *>(adjSeg + (size_t)k * sb);
+        v.v = v.x + nm;
+        v.F = reinterpret_cast<float *>(v.v + nm);
+        v.C = v.F + 9 * nm;
+        return v;
+    }
+
+    // Points the solver's particle state at `v` (the live arrays again for v = {}), returning what
+    // it pointed at.
+    Solver::StateView Solver::bindState(const StateView &v)
+    {
+        const StateView old{positionMass, velocity, F, Cm};
+        positionMass = v.x;
+        velocity = v.v;
+        F = v.F;
+        Cm = v.C;
+        return old;
+    }
+
+    // replay slot k: the forward substep runs on slot k as its state and writes slot k's tape; its
+    // G2P writes the updated state into slot k + 1, so slot k keeps the substep's input for the
+    // reverse pass without a copy (the segment's last slot: only up to the grid update)
     int Solver::replayBody(int k, size_t sb, bool last)
     {
-        int r = saveState(adjSeg + (size_t)k * sb);
-        if (r != CRB200_OK)
-            return r;
+        const StateView live = bindState(slotState(k, sb));
+        if (!last)
+        {
+            const StateView next = slotState(k + 1, sb);
+            outX = next.x;
+            outV = next.v;
+            outF = next.F;
+            outC = next.C;
+        }
         tapeActive = k;
-        r = last ? (isBatch() ? launchStepT<true>(true) : launchStepT<false>(true)) : launchStep();
+        const int r = last ? (isBatch() ? launchStepT<true>(true) : launchStepT<false>(true)) : launchStep();
         tapeActive = -1;
+        outX = outV = nullptr;
+        outF = outC = nullptr;
+        bindState(live);
         return r;
     }
 
@@ -1115,7 +1149,9 @@ namespace crb200
         adjReplayLastG.assign(K, nullptr);
         for (int k = 0; k < K; ++k)
         {
-            int r = captureGraph(0, k, &adjReplayG[k], &adjGraphKernels[0]);
+            // slot K-1 is always a segment's last substep: it has no full replay (which would write
+            // slot K)
+            int r = k + 1 < K ? captureGraph(0, k, &adjReplayG[k], &adjGraphKernels[0]) : CRB200_OK;
             if (r == CRB200_OK)
                 r = captureGraph(1, k, &adjReverseG[k], &adjGraphKernels[1]);
             if (r == CRB200_OK)
@@ -1142,9 +1178,15 @@ namespace crb200
         for (int seg = (T - 1) / K; seg >= 0; --seg)
         {
             const int t0 = seg * K, t1 = std::min(T, t0 + K);
-            // replay the segment's inputs s_t0 .. s_(t1-1), each substep writing its slot's tape
-            if ((r = loadState(adjCkpt + (size_t)seg * sb)) != CRB200_OK)
-                return r;
+            // replay the segment's inputs s_t0 .. s_(t1-1) in slots 0 .. t1-t0-1, each substep
+            // writing its slot's tape; the checkpoint is loaded into slot 0
+            {
+                const StateView live = bindState(slotState(0, sb));
+                r = loadState(adjCkpt + (size_t)seg * sb);
+                bindState(live);
+                if (r != CRB200_OK)
+                    return r;
+            }
             for (int t = t0; t < t1; ++t)
             {
                 const int k = t - t0;

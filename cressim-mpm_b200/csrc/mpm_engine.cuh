@@ -136,6 +136,15 @@ namespace crb200
         // solver-owned device state
         float *F = nullptr;  // 9 planes of numMaxParticles floats, F(r,c) in plane 3c + r
         float *Cm = nullptr; // APIC matrix, same layout
+        // where G2P writes the updated state when not in place (the adjoint's replay: the next
+        // tape slot); null in an ordinary substep
+        float4 *outX = nullptr, *outV = nullptr;
+        float *outF = nullptr, *outC = nullptr;
+        struct StateView
+        {
+            float4 *x = nullptr, *v = nullptr;
+            float *F = nullptr, *C = nullptr;
+        };
         float *V0 = nullptr;
         float4 *gridA = nullptr; // accumulation grid (zero outside a substep)
         float4 *gridV = nullptr; // velocity grid
@@ -199,6 +208,8 @@ namespace crb200
         unsigned adjGraphVersion = ~0u;
         unsigned char *adjGraphSeg = nullptr, *adjGraphTape = nullptr;
         int replayBody(int k, size_t sb, bool last);
+        StateView slotState(int k, size_t sb) const;
+        StateView bindState(const StateView &v);
         int reverseBody(int k, size_t sb);
         void releaseAdjoint();
         int adjointCheck();

@@ -983,8 +983,11 @@ namespace crb200
                                                  SortHeader *hdr, unsigned *__restrict__ keys,
                                                  unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
                                                  unsigned *__restrict__ cellCount,
-                                                 const unsigned long long *__restrict__ blockShapeMask)
+                                                 const unsigned long long *__restrict__ blockShapeMask,
+                                                 float4 *xo, float4 *vo, float *Fo, float *Co)
     {
+        // Modes 0 and 2 write the updated state to xo, vo, Fo, Co: the input arrays themselves in an
+        // ordinary substep, the next tape slot in the adjoint's replay (which keeps its input).
         // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
         // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
         if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)
@@ -1187,11 +1190,11 @@ namespace crb200
         for (int e = 0; e < 9; ++e)
             Mu.m[e] = ((e % 4) == 0 ? 1.f : 0.f) + Cn.m[e] * p.dt;
         Fp = matmul(Mu, Fp);
-        xm[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
-        vel[i] = make_float4(vn.x, vn.y, vn.z, 0.f);
-        storeM3(F, stride, i, Fp);
+        xo[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
+        vo[i] = make_float4(vn.x, vn.y, vn.z, 0.f);
+        storeM3(Fo, stride, i, Fp);
         if (Mode == 0)
-            storeM3(Cm, stride, i, Cn);
+            storeM3(Co, stride, i, Cn);
         if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)))
             atomicOr(status, CRB200_STATUS_NAN_STATE);
         if (kRecords && writeRecords && !(Multi && (sc.flags[si] & SF_SLICER)))
@@ -2076,7 +2079,9 @@ namespace crb200
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
                                                     (M == 0 || (M == 1 && pbRecords)) ? records : nullptr, gridA, header, keys, ranks,
-                                                    blockCount, cellCount, blockShapeMask);
+                                                    blockCount, cellCount, blockShapeMask,
+                                                    outX ? outX : positionMass, outX ? outV : velocity,
+                                                    outX ? outF : F, outX ? outC : Cm);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
