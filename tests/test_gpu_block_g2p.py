@@ -2,12 +2,11 @@
 
 Both compute each particle with the same source arithmetic; the block-ordered one gathers interior
 stencils from a shared-memory node tile.  With deterministic substeps (no order-dependent float
-sums anywhere) the two differ only by rounding, because the compiler may fuse multiply-adds
-(weights, stencil offsets) differently in the two kernels.  One substep: every output within 1e-5
-of its array's scale (1e-4 for C, a difference of nearly equal moments); after N substeps the
-positions within 1e-5 of theirs.  A node read from the wrong place would move velocities by their
-own size.  A particle given a non-finite position joins the scene's first cell, so the
-block-ordered G2P reaches it as the id-ordered one does."""
+sums anywhere) the two agree to float rounding: the compiler may fuse multiply-adds differently in
+the two kernels, which moves a few elements by an ulp.  So at least 99 % of every output is bit
+for bit equal and the rest within 1e-6 of the array's scale (a wrong node read would move
+positions by about v dt, 1e-5 m or more).  A particle given a non-finite position joins the
+scene's first cell, so the block-ordered G2P reaches it as the id-ordered one does."""
 import numpy as np
 import pytest
 
@@ -46,24 +45,20 @@ CASES = {
 }
 
 
-def _close(a, b, k, tol, case):
-    x, y = np.asarray(a[k], np.float64), np.asarray(b[k], np.float64)
-    finite = np.isfinite(y)
-    np.testing.assert_array_equal(np.isfinite(x), finite, err_msg=f"{case}: {k}")
-    scale = max(float(np.abs(y[finite]).max(initial=0.0)), 1e-12)
-    err = float(np.abs(x - y)[finite].max(initial=0.0))
-    assert err <= tol * scale, f"{case}: {k}: {err:.3e} against scale {scale:.3e}"
-
-
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_block_g2p_equals_id_order_g2p(case):
     make, steps = CASES[case]
     sc = make()
-    a, b = _run(sc, 1, True), _run(sc, 1, False)
-    for k, tol in (("x", 1e-5), ("v", 1e-5), ("F", 1e-5), ("C", 1e-4), ("force", 1e-5), ("torque", 1e-5)):
-        _close(a, b, k, tol, case)
-    a, b = _run(sc, steps, True), _run(sc, steps, False)
-    _close(a, b, "x", 1e-5, case)
+    a = _run(sc, steps, True)
+    b = _run(sc, steps, False)
+    for k in ("x", "v", "F", "C", "force", "torque"):
+        x, y = np.asarray(a[k], np.float64), np.asarray(b[k], np.float64)
+        finite = np.isfinite(y)
+        np.testing.assert_array_equal(np.isfinite(x), finite, err_msg=f"{case}: {k}")
+        same = (x == y) | ~finite
+        assert same.mean() >= 0.99, f"{case}: {k}: {same.mean():.4f} of the elements bit for bit equal"
+        scale = max(float(np.abs(y[finite]).max()), 1e-12) if finite.any() else 1.0
+        assert float(np.abs(x - y)[finite].max(initial=0.0)) <= 1e-6 * scale, f"{case}: {k}"
     if case == "nan_particle":
         # G2P clamps the non-finite position into the grid (fmin/fmax drop NaN operands)
         assert np.all(np.isfinite(a["x"][7]))
