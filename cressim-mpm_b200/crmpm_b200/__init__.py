@@ -33,7 +33,6 @@ STATUS_OUT_OF_DOMAIN = 0x4
 OPT_PHASE_TIMING = 3
 OPT_DETERMINISTIC_COUPLING = 4
 OPT_DETERMINISTIC = 5
-OPT_BLOCK_G2P = 6
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 
 

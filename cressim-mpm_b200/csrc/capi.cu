@@ -546,8 +546,6 @@ extern "C"
             if (int rc = s->setDeterministic(value != 0))
                 return rc;
         }
-        else if (option == CRB200_OPT_BLOCK_G2P)
-            s->blockG2P = value != 0;
         else
             return bad("CrB200SolverSetOption: unknown option");
         s->configVersion++;

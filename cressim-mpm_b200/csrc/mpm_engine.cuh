@@ -165,8 +165,6 @@ namespace crb200
         unsigned totalBlocks = 0;
         unsigned numTiles = 0;
         int p2gCtas = 0;
-        int g2pCtas = 0;        // persistent grid of k_g2pTiled
-        bool blockG2P = false; // CRB200_OPT_BLOCK_G2P
         int sortCtas = 0;
         int updCtas = 0;
         int strideCtas = 0;

@@ -299,12 +299,7 @@ namespace crb200
                 if (s.finite)
                     key = cellKey(g, s, &ood);
                 else
-                {
-                    // a non-finite position (given by the caller) still joins a block, the scene's
-                    // first cell, so that the block-ordered G2P reaches it; its P2G record is empty
-                    key = g.blockBase * 64u;
                     ood = true;
-                }
             }
         }
         const bool write = i < n && !carried;
@@ -976,126 +971,44 @@ namespace crb200
     //    particle (what k_record would compute from the stored state) unless a slicer is present,
     //    and mark the records valid; particles whose new stencil leaves the grid are scattered into
     //    the (cleared) accumulation grid here, as k_record does.
-    // Node sources of the interior G2P gather: the grid, or a block's 6x6x6 node tile in shared
-    // memory (tb: the stencil's base in the tile).
-    struct GridNodes
+    template <int Mode, bool Multi>
+    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : ((Mode == 0 && !Multi) ? 7 : 6)) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
+                                                 float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
+                                                 float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
+                                                 const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
+                                                 const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
+                                                 unsigned *status, const float4 *__restrict__ matParams,
+                                                 const int *__restrict__ matType, const float *__restrict__ V0,
+                                                 float4 *__restrict__ records, float4 *__restrict__ gridA,
+                                                 SortHeader *hdr, unsigned *__restrict__ keys,
+                                                 unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
+                                                 unsigned *__restrict__ cellCount,
+                                                 const unsigned long long *__restrict__ blockShapeMask,
+                                                 float4 *xo, float4 *vo, float *Fo, float *Co)
     {
-        const float4 *__restrict__ gridV;
-        unsigned AX[3], AY[3], AZ[3];
-        __device__ __forceinline__ V3 operator()(int a, int b, int c) const
-        {
-            return v3(__ldg(&gridV[AX[a] + AY[b] + AZ[c]]));
-        }
-    };
-    struct TileNodes
-    {
-        const float4 *tile;
-        int tb;
-        __device__ __forceinline__ V3 operator()(int a, int b, int c) const { return v3(tile[tb + a + 6 * b + 36 * c]); }
-    };
-    __device__ __forceinline__ V3 fmaV(V3 a, float s, V3 c)
-    {
-        return v3(__fmaf_rn(a.x, s, c.x), __fmaf_rn(a.y, s, c.y), __fmaf_rn(a.z, s, c.z));
-    }
-    __device__ __forceinline__ V3 mulV(V3 a, float s)
-    {
-        return v3(__fmul_rn(a.x, s), __fmul_rn(a.y, s), __fmul_rn(a.z, s));
-    }
-
-    // The interior MLS / PB G2P gather, S = sum w V and T[3r + c] = sum o_r (w V)_c: the weight
-    // is a product of 1D factors, so v and the offset moments contract axis by axis, over c
-    // (Z = sum w_c V, Zc = sum c w_c V), then b, then a.  The operations are spelled out
-    // (__fmaf_rn, __fmul_rn, __fadd_rn), so the sums do not depend on which source the nodes
-    // come from or on how the compiler would fuse them.
-    template <class Nodes>
-    __device__ __forceinline__ void gatherAxes(const float w[3][3], const Nodes &nodes, V3 &S, float T[9])
-    {
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-        {
-            V3 Y = v3(0.f, 0.f, 0.f), Yb = v3(0.f, 0.f, 0.f), Yc = v3(0.f, 0.f, 0.f);
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-            {
-                const V3 v0 = nodes(a, b, 0), v1 = nodes(a, b, 1), v2 = nodes(a, b, 2);
-                const V3 Zc = fmaV(v2, __fmul_rn(2.f, w[2][2]), mulV(v1, w[1][2]));
-                const V3 Z = fmaV(v2, w[2][2], fmaV(v1, w[1][2], mulV(v0, w[0][2])));
-                Y = fmaV(Z, w[b][1], Y);
-                if (b)
-                    Yb = fmaV(Z, __fmul_rn((float)b, w[b][1]), Yb);
-                Yc = fmaV(Zc, w[b][1], Yc);
-            }
-            const V3 wY = mulV(Y, w[a][0]);
-            S = v3(__fadd_rn(S.x, wY.x), __fadd_rn(S.y, wY.y), __fadd_rn(S.z, wY.z));
-            if (a)
-            {
-                T[0] = __fmaf_rn((float)a, wY.x, T[0]);
-                T[1] = __fmaf_rn((float)a, wY.y, T[1]);
-                T[2] = __fmaf_rn((float)a, wY.z, T[2]);
-            }
-            T[3] = __fmaf_rn(w[a][0], Yb.x, T[3]);
-            T[4] = __fmaf_rn(w[a][0], Yb.y, T[4]);
-            T[5] = __fmaf_rn(w[a][0], Yb.z, T[5]);
-            T[6] = __fmaf_rn(w[a][0], Yc.x, T[6]);
-            T[7] = __fmaf_rn(w[a][0], Yc.y, T[7]);
-            T[8] = __fmaf_rn(w[a][0], Yc.z, T[8]);
-        }
-    }
-
-    // The pointers of one G2P launch (k_g2p, k_g2pTiled).
-    struct G2PArgs
-    {
-        float4 *xm, *vel;
-        float *F, *Cm;
-        unsigned stride;
-        const ShapeRec *shapeTable;
-        SdfPtrs sdf;
-        const float4 *gridV;
-        const unsigned *cutMasks;
-        unsigned *status;
-        const float4 *matParams;
-        const int *matType;
-        const float *V0;
-        float4 *records, *gridA;
-        SortHeader *hdr;
-        unsigned *keys, *ranks, *blockCount, *cellCount;
-        const unsigned long long *blockShapeMask;
-        float4 *xo, *vo;
-        float *Fo, *Co;
-    };
-
-    // G2P of particle i (scene si), the body of k_g2p and k_g2pTiled.  Tiled: an interior stencil
-    // based inside the 4x4x4 block whose 6x6x6 node tile (origin tox, toy, toz) is in shared
-    // memory gathers from the tile, with the same arithmetic as from the grid.
-    template <int Mode, bool Multi, bool Tiled>
-    __device__ __forceinline__ void g2pParticle(const StepParams &p0, SceneTable sc, G2PArgs A, const ShapeRec *sh,
-                                                unsigned i, unsigned si, bool writeRecords, const float4 *tile,
-                                                int tox, int toy, int toz)
-    {
+        // Modes 0 and 2 write the updated state to xo, vo, Fo, Co: the input arrays themselves in an
+        // ordinary substep, the next tape slot in the adjoint's replay (which keeps its input).
+        // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
+        // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
+        if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)
+            hdr->pbRecordsValid = records != nullptr ? 1u : 0u; // read only by later launches
         constexpr bool kRecords = Mode == 0;
-        float4 *__restrict__ xm = A.xm;
-        float4 *__restrict__ vel = A.vel;
-        float *__restrict__ F = A.F;
-        float *__restrict__ Cm = A.Cm;
-        const unsigned stride = A.stride;
-        const ShapeRec *__restrict__ shapeTable = A.shapeTable;
-        const SdfPtrs sdf = A.sdf;
-        const float4 *__restrict__ gridV = A.gridV;
-        const unsigned *__restrict__ cutMasks = A.cutMasks;
-        unsigned *status = A.status;
-        const float4 *__restrict__ matParams = A.matParams;
-        const int *__restrict__ matType = A.matType;
-        const float *__restrict__ V0 = A.V0;
-        float4 *__restrict__ records = A.records;
-        float4 *__restrict__ gridA = A.gridA;
-        SortHeader *hdr = A.hdr;
-        unsigned *__restrict__ keys = A.keys;
-        unsigned *__restrict__ ranks = A.ranks;
-        unsigned *__restrict__ blockCount = A.blockCount;
-        unsigned *__restrict__ cellCount = A.cellCount;
-        const unsigned long long *__restrict__ blockShapeMask = A.blockShapeMask;
-        float4 *xo = A.xo, *vo = A.vo;
-        float *Fo = A.Fo, *Co = A.Co;
+        const bool writeRecords =
+            kRecords && records != nullptr && (Multi || !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER)));
+        if (writeRecords && blockIdx.x == 0 && threadIdx.x == 0)
+            hdr->recordsValid = 1u; // read only by later launches
+        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
+        if (!Multi && p0.numShapes > 0)
+        {
+            loadShapes(sh, shapeTable, p0.numShapes);
+            __syncthreads();
+        }
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
+            return;
+        const unsigned si = Multi ? sc.particleScene[i] : 0u;
+        if (Multi && si == 0xFFFFu)
+            return;
         const StepParams &p = Multi ? sc.params[si] : p0;
         const GridGeom &g = p.g;
         const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
@@ -1135,9 +1048,6 @@ namespace crb200
                     AY[e] = (unsigned)(((g.nb.x * (yi >> 2)) << 6) + 4 * (yi & 3));
                     AZ[e] = (unsigned)(((g.nb.x * g.nb.y * (zi >> 2)) << 6) + 16 * (zi & 3));
                 }
-                // Tiled: a stencil based inside the tile's 4x4x4 block reads the node tile
-                const int tx = st.b[0] - tox, ty = st.b[1] - toy, tz = st.b[2] - toz;
-                const bool inTile = Tiled && tx >= 0 && tx <= 3 && ty >= 0 && ty <= 3 && tz >= 0 && tz <= 3;
                 if (Mode == 2)
                 {
 #pragma unroll
@@ -1148,10 +1058,43 @@ namespace crb200
                             for (int c = 0; c < 3; ++c)
                                 g2pNode<Mode>(a, b, c, v3(__ldg(&gridV[AX[a] + AY[b] + AZ[c]])), w, dw, S, T);
                 }
-                else if (Tiled && inTile)
-                    gatherAxes(w, TileNodes{tile, tx + 6 * ty + 36 * tz}, S, T);
                 else
-                    gatherAxes(w, GridNodes{gridV, {AX[0], AX[1], AX[2]}, {AY[0], AY[1], AY[2]}, {AZ[0], AZ[1], AZ[2]}}, S, T);
+                {
+                    // The weight is a product of 1D factors, so v and the offset moments contract
+                    // axis by axis: over c (Z = sum w_c V, Zc = sum c w_c V), then b, then a.
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        V3 Y = v3(0.f, 0.f, 0.f), Yb = v3(0.f, 0.f, 0.f), Yc = v3(0.f, 0.f, 0.f);
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                        {
+                            const unsigned ab = AX[a] + AY[b];
+                            const V3 v0 = v3(__ldg(&gridV[ab + AZ[0]])), v1 = v3(__ldg(&gridV[ab + AZ[1]])),
+                                     v2 = v3(__ldg(&gridV[ab + AZ[2]]));
+                            const V3 Zc = v1 * w[1][2] + v2 * (2.f * w[2][2]);
+                            const V3 Z = v0 * w[0][2] + v1 * w[1][2] + v2 * w[2][2];
+                            Y = Y + Z * w[b][1];
+                            if (b)
+                                Yb = Yb + Z * ((float)b * w[b][1]);
+                            Yc = Yc + Zc * w[b][1];
+                        }
+                        const V3 wY = Y * w[a][0];
+                        S = S + wY;
+                        if (a)
+                        {
+                            T[0] += (float)a * wY.x;
+                            T[1] += (float)a * wY.y;
+                            T[2] += (float)a * wY.z;
+                        }
+                        T[3] += w[a][0] * Yb.x;
+                        T[4] += w[a][0] * Yb.y;
+                        T[5] += w[a][0] * Yb.z;
+                        T[6] += w[a][0] * Yc.x;
+                        T[7] += w[a][0] * Yc.y;
+                        T[8] += w[a][0] * Yc.z;
+                    }
+                }
             }
             else
             {
@@ -1294,101 +1237,6 @@ namespace crb200
             binAggregated(am, lane, key, blockCount, cellCount, &keys[i], &ranks[i]);
             if (__any_sync(am, ood) && (int)lane == __ffs(am) - 1)
                 atomicOr(&hdr->status, CRB200_STATUS_OUT_OF_DOMAIN);
-        }
-    }
-
-    template <int Mode, bool Multi>
-    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : ((Mode == 0 && !Multi) ? 7 : 6)) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
-                                                 float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
-                                                 float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
-                                                 const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
-                                                 const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
-                                                 unsigned *status, const float4 *__restrict__ matParams,
-                                                 const int *__restrict__ matType, const float *__restrict__ V0,
-                                                 float4 *__restrict__ records, float4 *__restrict__ gridA,
-                                                 SortHeader *hdr, unsigned *__restrict__ keys,
-                                                 unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
-                                                 unsigned *__restrict__ cellCount,
-                                                 const unsigned long long *__restrict__ blockShapeMask,
-                                                 float4 *xo, float4 *vo, float *Fo, float *Co)
-    {
-        // Modes 0 and 2 write the updated state to xo, vo, Fo, Co: the input arrays themselves in an
-        // ordinary substep, the next tape slot in the adjoint's replay (which keeps its input).
-        // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
-        // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
-        if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)
-            hdr->pbRecordsValid = records != nullptr ? 1u : 0u; // read only by later launches
-        constexpr bool kRecords = Mode == 0;
-        const bool writeRecords =
-            kRecords && records != nullptr && (Multi || !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER)));
-        if (writeRecords && blockIdx.x == 0 && threadIdx.x == 0)
-            hdr->recordsValid = 1u; // read only by later launches
-        __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
-        if (!Multi && p0.numShapes > 0)
-        {
-            loadShapes(sh, shapeTable, p0.numShapes);
-            __syncthreads();
-        }
-        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= (Multi ? sc.numParticles : p0.numActive) || !mask[i])
-            return;
-        const unsigned si = Multi ? sc.particleScene[i] : 0u;
-        if (Multi && si == 0xFFFFu)
-            return;
-        const G2PArgs A{xm, vel, F, Cm, stride, shapeTable, sdf, gridV, cutMasks, status, matParams, matType, V0,
-                         records, gridA, hdr, keys, ranks, blockCount, cellCount, blockShapeMask, xo, vo, Fo, Co};
-        g2pParticle<Mode, Multi, false>(p0, sc, A, sh, i, si, writeRecords, nullptr, 0, 0, 0);
-    }
-
-    // MLS G2P of one scene over the sorted particles of each active 4x4x4 block (this substep's
-    // sort: positions change only here).  The block's 6x6x6 node tile of grid velocities is
-    // staged in shared memory once, and the interior stencils based in the block gather from it;
-    // every other particle takes k_g2p's path.  Same arithmetic as k_g2p (the two agree to float
-    // rounding: the compiler may fuse multiply-adds differently in the two kernels).
-    __global__ void __launch_bounds__(128, 6) k_g2pTiled(
-        const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm, float4 *__restrict__ vel,
-        const unsigned char *__restrict__ mask, float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
-        const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf, const float4 *__restrict__ gridV,
-        const unsigned *__restrict__ cutMasks, unsigned *status, const float4 *__restrict__ matParams,
-        const int *__restrict__ matType, const float *__restrict__ V0, float4 *__restrict__ records,
-        float4 *__restrict__ gridA, SortHeader *hdr, unsigned *__restrict__ keys, unsigned *__restrict__ ranks,
-        unsigned *__restrict__ blockCount, unsigned *__restrict__ cellCount,
-        const unsigned long long *__restrict__ blockShapeMask, float4 *xo, float4 *vo, float *Fo, float *Co,
-        const unsigned *__restrict__ activeList, const unsigned *__restrict__ blockStart,
-        const unsigned *__restrict__ sortedIds)
-    {
-        const bool writeRecords = records != nullptr && !(p0.numShapes > 0 && (sc.flags[0] & SF_SLICER));
-        if (writeRecords && blockIdx.x == 0 && threadIdx.x == 0)
-            hdr->recordsValid = 1u; // read only by later launches
-        __shared__ ShapeRec sh[kMaxShapes];
-        __shared__ float4 tile[216];
-        if (p0.numShapes > 0)
-            loadShapes(sh, shapeTable, p0.numShapes);
-        const G2PArgs A{xm, vel, F, Cm, stride, shapeTable, sdf, gridV, cutMasks, status, matParams, matType, V0,
-                         records, gridA, hdr, keys, ranks, blockCount, cellCount, blockShapeMask, xo, vo, Fo, Co};
-        const GridGeom &g = p0.g;
-        // set by the sort that ran before this launch (G2P's binning updates only the counts)
-        const unsigned nAct = hdr->numActiveBlocks;
-        for (unsigned ab = blockIdx.x; ab < nAct; ab += gridDim.x)
-        {
-            const unsigned b = activeList[ab];
-            const unsigned lb = b - g.blockBase;
-            const int ox = 4 * (int)(lb % g.nb.x), oy = 4 * (int)((lb / g.nb.x) % g.nb.y),
-                      oz = 4 * (int)(lb / (g.nb.x * g.nb.y));
-            __syncthreads(); // the previous block's tile is no longer read (and the shapes are loaded)
-            for (int t = threadIdx.x; t < 216; t += blockDim.x)
-            {
-                const int ni = ox + t % 6, nj = oy + (t / 6) % 6, nk = oz + t / 36;
-                tile[t] = inGrid(g, ni, nj, nk) ? __ldg(&gridV[nodeAddr(g, ni, nj, nk)]) : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            __syncthreads();
-            const unsigned start = blockStart[b], cnt = blockStart[b + 1] - start;
-            for (unsigned q = threadIdx.x; q < cnt; q += blockDim.x)
-            {
-                const unsigned i = sortedIds[start + q];
-                if (mask[i])
-                    g2pParticle<0, false, true>(p0, sc, A, sh, i, 0u, writeRecords, tile, ox, oy, oz);
-            }
         }
     }
 
@@ -2035,8 +1883,6 @@ namespace crb200
         CRB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_accumulate<0, false>, 64, 0));
         p2gCtas = sms * (perSm > 0 ? perSm : 1);
-        CRB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_g2pTiled, 128, 0));
-        g2pCtas = sms * (perSm > 0 ? perSm : 1);
         sortCtas = sms * 4;  // 64-thread CTAs of the on-request sort-state kernel
         cellCtas = sms * 4;  // 256-thread CTAs of k_cellStarts (one warp per active block)
         updCtas = sms * 8;
@@ -2230,17 +2076,6 @@ namespace crb200
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
-            if constexpr (!Multi && M == 0)
-                if (blockG2P)
-                {
-                    k_g2pTiled<<<std::max(1, std::min(g2pCtas, (int)totalBlocks)), 128, 0, stream>>>(
-                        p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable, sp, gridV, cutMasks,
-                        &header->status, matParams, matType, V0, records, gridA, header, keys, ranks, blockCount,
-                        cellCount, blockShapeMask, outX ? outX : positionMass, outX ? outV : velocity, outX ? outF : F,
-                        outX ? outC : Cm, activeList, blockStart, sortedIds);
-                    CRB_LAUNCHED(1);
-                    return CRB200_OK;
-                }
             k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
                                                     (M == 0 || (M == 1 && pbRecords)) ? records : nullptr, gridA, header, keys, ranks,

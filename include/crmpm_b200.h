@@ -280,11 +280,6 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
  * Single-scene solvers only; the substeps an adjoint backward pass replays use the ordinary path. */
 #define CRB200_OPT_DETERMINISTIC 5
-/* CRB200_OPT_BLOCK_G2P (off by default): the MLS G2P of a single-scene solver walks the sorted
- * particles of each active 4x4x4 cell block and gathers the grid velocities of interior stencils
- * from the block's 6x6x6 node tile in shared memory; off, it walks the particles in id order and
- * gathers from the grid.  Both evaluate the same arithmetic and agree to float rounding. */
-#define CRB200_OPT_BLOCK_G2P 6
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the
