@@ -451,7 +451,7 @@ def run_ours(args, rank, world, local):
     probe = scene.shapes.shape_ids[-1]  # the moving shape (probe or blade), moved along its velocity
     pose0 = ds.sh["position"][probe].cpu()
     probe_vel = scene.shapes.lin_vel[probe, :3].astype(np.float64)
-    frames = max(3, args.steps // frame_substeps)
+    frames = max(20, args.steps // frame_substeps)
     # one pinned pose per frame: a frame's upload may still be queued when the next is written
     poses = [torch.empty(4, dtype=torch.float32, pin_memory=True) for _ in range(frames)]
     for f_ in range(frames):
@@ -502,6 +502,11 @@ def run_ours(args, rank, world, local):
                    "sample": f"{done} substeps of the same workload ({scene.n} particles, {el:.1f} s) with the reference's "
                              f"serial CPU solver arithmetic built from its own headers"}
     status = s.status()
+    extras = None
+    if args.workload == "slab" and world == 1 and not args.no_extras:
+        del ds
+        torch.cuda.synchronize(dev)
+        extras = bench_extras(args, local, scene, value)
     out = {
         "metric": METRICS[args.workload] + (" deterministic" if args.deterministic else ""),
         "value": value,
@@ -533,28 +538,100 @@ def run_ours(args, rank, world, local):
         out["deterministic"] = det
     if cpu is not None:
         out["cpu_baseline"] = cpu
+    if extras is not None:
+        out.update(extras)
     return out
 
 
-def run_batch(args, rank, world, local):
-    """256 batched scenes vs the same scenes one by one on the plain solver."""
+def bench_extras(args, local, slab_scene, slab_value):
+    """The engine's other targets, each timed outside the headline's timed region with CUDA events
+    on its own stream and bounded to a few seconds of GPU work, so that a default run reports them:
+
+    * reference_gpu: the reference's own CUDA solver on the slab over 200 substeps (the >= 3x bar);
+    * batch: the 256-scene batch against the same scenes one by one on the plain solver (>= 2x);
+    * adjoint: backward over plain forward for the 64k cube and a 64-scene batch of it (<= 3x);
+    * pb: the PB-MPM cutting workload against the reference's CUDA solver on the same scene.
+    A part that fails reports its error instead of stopping the run."""
     import torch
 
     import crmpm_b200 as cb
     from crmpm_b200 import scenes
 
-    cb.build_library()
     dev = f"cuda:{local}"
-    torch.cuda.set_device(local)
+    out = {}
+
+    def guard(name, fn):
+        try:
+            out[name] = fn()
+        except Exception as e:  # noqa: BLE001 - reported in the line, the headline stands
+            out[name] = {"error": f"{type(e).__name__}: {str(e).splitlines()[0][:200] if str(e) else ''}"}
+        torch.cuda.synchronize(dev)
+
+    def ref_slab():
+        r = reference_gpu_run(slab_scene, args, steps=200)
+        if r is not None and "value" in r:
+            r["engine_over_reference"] = slab_value / r["value"]
+        return r
+
+    def batch():
+        r = batch_measure(20, 3, 0, 1, local)
+        return {"value": r["value"], "unit": "particle-substeps/s", "substeps": 20, "scenes": len(r["sl"]),
+                "particles": r["n"], "one_by_one": r["one_value"], "one_by_one_substeps": r["k1"],
+                "batch_over_one_by_one": r["value"] / r["one_value"],
+                "how": "one batch solver (one launch per phase, CUDA graph) vs one plain solver per scene on a "
+                       "shared stream (CUDA graph per scene)"}
+
+    def adjoint():
+        T, single, b64 = adjoint_measure(local)
+        return {"workload": ADJOINT_CONFIG, "substeps": T, "single": single, "batch64": b64,
+                "target": "backward <= 3x the plain forward"}
+
+    def pb():
+        sc = scenes.pb_cutting()
+        ds = cb.DeviceScene(sc, device=dev)
+        ds.step(3)
+        ds.sync()
+        steps = 20
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ds.stream)
+        ds.solver.step_many(steps)
+        e1.record(ds.stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        del ds
+        r = {"value": sc.n / (ms / 1e3), "unit": "particle-steps/s", "ms_per_step": ms, "steps": steps,
+             "particles": sc.n, "iterations": sc.iterations}
+        ref = reference_gpu_run(sc, args, steps=steps)
+        if ref is not None:
+            r["reference_gpu"] = ref
+            if "value" in ref:
+                r["engine_over_reference"] = r["value"] / ref["value"]
+        return r
+
+    guard("reference_gpu", ref_slab)
+    guard("batch", batch)
+    guard("adjoint", adjoint)
+    guard("pb", pb)
+    return out
+
+
+def batch_measure(steps, warmup, rank, world, local, sampler=None):
+    """256 batched scenes (this rank's shard) stepped by one batch solver, then the same scenes one
+    by one on plain single-scene solvers; CUDA events on each stream, max over ranks."""
+    import torch
+
+    import crmpm_b200 as cb
+    from crmpm_b200 import scenes
     from crmpm_b200.sharding import shard_scenes
 
+    dev = f"cuda:{local}"
     sl_all = scenes.batched_scenes()
     # N GPUs: each rank steps its own scenes (largest-first balance), no data-path collective
     mine = shard_scenes([sc.n for sc in sl_all], world)[rank]
     sl = [sl_all[k] for k in mine]
     n = sum(sc.n for sc in sl_all)
     b = cb.DeviceBatch(sl, device=dev)
-    b.step(max(args.warmup, 3))
+    b.step(max(warmup, 3))
     tuned = b.solver.autotune(4)
     b.step(2)
     b.sync()
@@ -571,26 +648,46 @@ def run_batch(args, rank, world, local):
         e1.synchronize()
         return max_over_ranks(e0.elapsed_time(e1), world)
 
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
+    if sampler is not None:
+        sampler.start()
+        time.sleep(0.3)
     launches0 = cb.kernel_launch_count()
-    ms = timed(b.stream, lambda: b.solver.step_many(args.steps))
+    ms = timed(b.stream, lambda: b.solver.step_many(steps))
     launches = cb.kernel_launch_count() - launches0
-    clocks = sampler.stop()
-    value = n * args.steps / (ms / 1e3)
+    clocks = sampler.stop() if sampler is not None else None
+    value = n * steps / (ms / 1e3)
+    status = b.solver.status()
+    del b
 
     # one by one: a plain solver per scene, all on one stream, each scene's substeps in turn
     shared = torch.cuda.Stream(device=dev)
     singles = [cb.DeviceScene(sc, device=dev, stream=shared) for sc in sl]
     for g in singles:
         g.step(3)
-    k1 = min(args.steps, 50)
+    k1 = min(steps, 50)
     ms1 = timed(shared, lambda: [g.solver.step_many(k1) for g in singles])
     one_value = n * k1 / (ms1 / 1e3)
+    del singles
     peak, peak_kind = hbm_peak()
     n_mine = sum(sc.n for sc in sl)
-    substep_gbs = (200.0 * n_mine + 64.0 * touched_nodes) / (ms / 1e3 / args.steps) / 1e9
+    substep_gbs = (200.0 * n_mine + 64.0 * touched_nodes) / (ms / 1e3 / steps) / 1e9
+    return dict(n=n, sl=sl, ms=ms, value=value, one_value=one_value, k1=k1, tuned=tuned, launches=launches,
+                clocks=clocks, touched_nodes=touched_nodes, substep_gbs=substep_gbs, peak=peak, peak_kind=peak_kind,
+                status=status)
+
+
+def run_batch(args, rank, world, local):
+    """256 batched scenes vs the same scenes one by one on the plain solver."""
+    import torch
+
+    import crmpm_b200 as cb
+
+    cb.build_library()
+    torch.cuda.set_device(local)
+    r = batch_measure(args.steps, args.warmup, rank, world, local, sampler=ClockSampler(local))
+    n, sl, ms, value, one_value, k1 = r["n"], r["sl"], r["ms"], r["value"], r["one_value"], r["k1"]
+    tuned, launches, clocks, touched_nodes = r["tuned"], r["launches"], r["clocks"], r["touched_nodes"]
+    substep_gbs, peak, peak_kind = r["substep_gbs"], r["peak"], r["peak_kind"]
     return {
         "metric": "particle-substeps/s (batched MLS-MPM, 256 scenes)",
         "value": value,
@@ -616,23 +713,27 @@ def run_batch(args, rank, world, local):
                      "unit": "GB/s", "frac": substep_gbs / peak, "peak_source": peak_kind},
         "gpu_launches": int(launches),
         "clocks": clocks,
-        "status": b.solver.status(),
+        "status": r["status"],
     }
 
 
-def run_adjoint(args, rank, world, local):
-    """Material identification: forward record + adjoint of the 64k-particle cube (and a 64-scene batch)."""
+ADJOINT_CONFIG = ("64k-particle Neo-Hookean cube (0.4 m, dx 0.02, 8 ppc) 1 cm above a ground plane at -1 m/s, 200 "
+                  "substeps of 2e-4 s, positions captured at 50/100/150/200, checkpoint every 20; gradients at E 8e3, "
+                  "nu 0.25 against targets made at E 2e4, nu 0.35")
+
+
+def adjoint_measure(local, quick=False, with_batch=True):
+    """Forward record + backward of the material-identification cube (and of a 64-scene batch of
+    it), each against the plain forward of the same substeps; CUDA events on the solver stream."""
     import torch
 
     import crmpm_b200 as cb
     from crmpm_b200 import scenes
     from crmpm_b200.adjoint import Trajectory, lame
 
-    cb.build_library()
     dev = f"cuda:{local}"
-    torch.cuda.set_device(local)
     T, caps, K = 200, (50, 100, 150, 200), 20
-    if args.quick:  # short run for profiler launch lists: 40 substeps, the single cube only
+    if quick:  # short run for profiler launch lists: 40 substeps, the single cube only
         T, caps, K = 40, (20, 40), 20
 
     def cube(seed):
@@ -672,7 +773,21 @@ def run_adjoint(args, rank, world, local):
                     backward_over_plain_forward=bwd / plain, grad_E_sign_check=float(gl.sum()))
 
     single = measure(cb.DeviceScene(cube(1005), device=dev), None)
-    batch = None if args.quick else measure(cb.DeviceBatch([cube(2000 + s) for s in range(64)], device=dev), None)
+    batch = None
+    if with_batch and not quick:
+        batch = measure(cb.DeviceBatch([cube(2000 + s) for s in range(64)], device=dev), None)
+    return T, single, batch
+
+
+def run_adjoint(args, rank, world, local):
+    """Material identification: forward record + adjoint of the 64k-particle cube (and a 64-scene batch)."""
+    import torch
+
+    import crmpm_b200 as cb
+
+    cb.build_library()
+    torch.cuda.set_device(local)
+    T, single, batch = adjoint_measure(local, quick=args.quick)
     n = single["particles"]
     value = n * T / (single["backward_ms"] / 1e3)
     return {
@@ -688,9 +803,7 @@ def run_adjoint(args, rank, world, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded jittered particles)",
-        "config": {"workload": "64k-particle Neo-Hookean cube (0.4 m, dx 0.02, 8 ppc) 1 cm above a ground plane at "
-                               "-1 m/s, 200 substeps of 2e-4 s, positions captured at 50/100/150/200, checkpoint "
-                               "every 20; gradients at E 8e3, nu 0.25 against targets made at E 2e4, nu 0.35"},
+        "config": {"workload": ADJOINT_CONFIG},
         "single": single,
         "batch64": batch,
     }
@@ -742,7 +855,7 @@ def run_reference(args, rank, world):
     return line
 
 
-def reference_gpu_run(scene, args):
+def reference_gpu_run(scene, args, steps=None):
     """The reference's own CUDA solver (oracle/_ref/ref_gpu_driver: src/solver/gpu_*_mpm_solver.cu
     built for sm_100a) on the same workload, timed with CUDA events on its stream after warm-up
     substeps, inputs resident in HBM.  None when the driver is not built."""
@@ -751,7 +864,8 @@ def reference_gpu_run(scene, args):
 
     if not op.ref_gpu_available():
         return None
-    steps = min(args.steps, 500 if scene.solver_type != 3 else 100)
+    if steps is None:
+        steps = min(max(args.steps, 200), 500 if scene.solver_type != 3 else 100)
     try:
         r = op.ref_gpu_run(scene, steps, warmup=max(args.warmup, 3))
     except (RuntimeError, OSError, subprocess.TimeoutExpired) as e:
@@ -776,6 +890,8 @@ def main():
                     help="single-scene workloads: run the timed substeps with CRB200_OPT_DETERMINISTIC on")
     ap.add_argument("--quick", action="store_true",
                     help="timed region only (no phase pass, e2e or CPU baseline): for profiler launch lists")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="slab workload: skip the batch / adjoint / PB / reference-GPU figures after the headline")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

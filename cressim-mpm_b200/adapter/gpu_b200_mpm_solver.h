@@ -1,7 +1,7 @@
 // Drop-in solver for CRESSim-MPM: a MpmSolverGpu (src/solver/mpm_solver_gpu.h:43-57) whose every
 // MpmSolver member (include/solver/mpm_solver.h:63-191) forwards to libcrmpm_b200.so.
 //
-// This header is compiled inside the reference's engine target (see INTEGRATION.md): it includes
+// This header is compiled inside the reference's engine target: it includes
 // the reference's own solver headers, and SimulationFactoryImpl::createScene
 // (src/engine/simulation_factory_impl.cpp:296-349) constructs it in place of GpuMlsMpmSolver,
 // GpuPbMpmSolver or GpuStandardMpmSolver.  The factory sets the CUDA stream before initialize()

@@ -972,9 +972,9 @@ namespace crb200
     //    and mark the records valid; particles whose new stencil leaves the grid are scattered into
     //    the (cleared) accumulation grid here, as k_record does.
     template <int Mode, bool Multi>
-    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : ((Mode == 0 && !Multi) ? 7 : 6)) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *__restrict__ xm,
-                                                 float4 *__restrict__ vel, const unsigned char *__restrict__ mask,
-                                                 float *__restrict__ F, float *__restrict__ Cm, unsigned stride,
+    __global__ void __launch_bounds__(128, Mode == 1 ? 4 : ((Mode == 0 && !Multi) ? 7 : 6)) k_g2p(const __grid_constant__ StepParams p0, SceneTable sc, float4 *xm,
+                                                 float4 *vel, const unsigned char *__restrict__ mask,
+                                                 float *F, float *Cm, unsigned stride,
                                                  const ShapeRec *__restrict__ shapeTable, SdfPtrs sdf,
                                                  const float4 *__restrict__ gridV, const unsigned *__restrict__ cutMasks,
                                                  unsigned *status, const float4 *__restrict__ matParams,
@@ -988,6 +988,8 @@ namespace crb200
     {
         // Modes 0 and 2 write the updated state to xo, vo, Fo, Co: the input arrays themselves in an
         // ordinary substep, the next tape slot in the adjoint's replay (which keeps its input).
+        // Inputs and outputs may therefore alias, so none of xm, vel, F, Cm, xo, vo, Fo, Co is
+        // declared __restrict__; each thread reads its own particle before it writes it.
         // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
         // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
         if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)

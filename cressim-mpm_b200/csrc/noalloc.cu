@@ -15,13 +15,17 @@
 //   * all calls share the one scratch array, so two calls that overlap on the GPU (different
 //     streams, or different host threads) race and corrupt each other's grids: serialise them;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress with
-//     that device current); make that first call before any stream capture.
+//     that device current); make that first call before any stream capture.  The address is kept
+//     for the life of the process, so a device reset (cudaDeviceReset, or anything else that
+//     destroys the primary context) after that first call is not supported: later calls would
+//     use an address of the destroyed context.
 // The arithmetic is the regular MLS substep (mls_mpm_algorithm.h:147-390 of the reference):
 // per-particle P2G with float4 vector atomics into a dense grid, the grid update with SDF contact
 // and domain boundary, and G2P; only the grid layout (dense, x fastest) and the scratch source
 // differ, so results agree with CrB200SolverStep to float32 rounding.
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 #include <mutex>
 
@@ -402,10 +406,35 @@ extern "C" CRB200_API int CrB200MlsSubstepNoAlloc(const CrB200NoAllocStep *step,
         setLastError("CrB200MlsSubstepNoAlloc: null particle buffer");
         return CRB200_ERR_INVALID_ARGUMENT;
     }
-    if (s.numShapes > 0 && (!s.shapeIds || !s.shapes.type || !s.geometries.type))
+    if (s.numShapes > 0 &&
+        (!s.shapeIds || !s.shapes.type || !s.shapes.geometryIdx || !s.shapes.position || !s.shapes.rotation ||
+         !s.shapes.invScale || !s.shapes.linearVelocity || !s.shapes.angularVelocity || !s.shapes.params0 ||
+         !s.shapes.force || !s.shapes.torque || !s.geometries.type || !s.geometries.params0))
     {
-        setLastError("CrB200MlsSubstepNoAlloc: shapes enabled but shape ids / shape data / geometry data are null");
+        setLastError("CrB200MlsSubstepNoAlloc: shapes enabled but shape ids or a shape / geometry array the substep "
+                     "reads or writes (type, geometryIdx, position, rotation, invScale, linearVelocity, "
+                     "angularVelocity, params0, force, torque; geometry type, params0) is null");
         return CRB200_ERR_INVALID_ARGUMENT;
+    }
+    // the kernels read these arrays as float4: an address off a 16-byte boundary would be a
+    // misaligned access on the GPU, so it is refused here (as CrB200SolverBindParticleData does)
+    {
+        const void *vec4[] = {s.positionMass, s.velocity, s.matParams};
+        for (const void *q : vec4)
+            if (s.numParticles > 0 && (reinterpret_cast<uintptr_t>(q) & 15u) != 0)
+            {
+                setLastError("CrB200MlsSubstepNoAlloc: positionMass, velocity and matParams must be 16-byte aligned");
+                return CRB200_ERR_INVALID_ARGUMENT;
+            }
+        const void *shape4[] = {s.shapes.position, s.shapes.rotation, s.shapes.invScale, s.shapes.linearVelocity,
+                                s.shapes.angularVelocity, s.shapes.params0, s.shapes.force, s.shapes.torque,
+                                s.shapes.comInvMass, s.shapes.inertiaInv0, s.shapes.inertiaInv1, s.geometries.params0};
+        for (const void *q : shape4)
+            if (s.numShapes > 0 && (reinterpret_cast<uintptr_t>(q) & 15u) != 0)
+            {
+                setLastError("CrB200MlsSubstepNoAlloc: shape and geometry float4 arrays must be 16-byte aligned");
+                return CRB200_ERR_INVALID_ARGUMENT;
+            }
     }
     noalloc::DevicePtrs ptrs;
     int rc = noalloc::devicePtrs(ptrs);

@@ -403,8 +403,14 @@ typedef struct CrB200NoAllocStep {
  * static device array of 2 x 262,144 nodes (8 MiB), held by every GPU that loads the library:
  * grids above 262,144 nodes (or more than 64 shapes) are rejected with CRB200_ERR_CAPACITY.  All
  * calls share that array, so calls that overlap on the GPU race; serialise them.  The first call on
- * a device looks up the array's address and should come before any stream capture.  The substep
- * is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * a device looks up the array's address and should come before any stream capture; that address
+ * is kept for the life of the process, so resetting the device afterwards is not supported.
+ * positionMass, velocity, matParams and the shape / geometry float4 arrays must be 16-byte
+ * aligned, and with shapes every shape array the substep reads (type, geometryIdx, position,
+ * rotation, invScale, linearVelocity, angularVelocity, params0) and writes (force, torque) must be
+ * non-null (CRB200_ERR_INVALID_ARGUMENT otherwise).  Every shapeIds entry must lie in
+ * [0, shapes.size) and every geometryIdx in [0, geometries.size), as for the regular solver.  The
+ * substep is enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
 CRB200_API int CrB200MlsSubstepNoAlloc(const CrB200NoAllocStep *step, void *stream);
 
 /* ------------------------------------------------------------------------------------------ */

@@ -38,12 +38,22 @@ class GeometrySdfDataC(C.Structure):
     _fields_ = [("dimension", C.c_void_p), ("lowerBoundCellSize", C.c_void_p), ("gradientSignedDistance", C.c_void_p)]
 
 
+def reference_root() -> str | None:
+    """Where the reference's sources lie, as the oracle recipe (oracle/Makefile, `print-ref`) has
+    it; None when that folder does not exist (on a machine that only runs the prebuilt oracle)."""
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True, check=True)
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    path = r.stdout.strip()
+    return path if path and os.path.isdir(path) else None
+
+
 def build(ref: bool = True) -> None:
     """Compile the restatement (and, when the reference sources exist, the reference driver)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    if ref and os.path.isdir(os.environ.get("CRMPM_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={os.environ.get('CRMPM_REFERENCE', '/root/reference')}"],
-                       check=True)
+    if ref and reference_root() is not None:
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
 def ref_available() -> bool:

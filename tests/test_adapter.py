@@ -10,10 +10,13 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("CRMPM_REFERENCE", "/root/reference")
+import oracle_py  # noqa: E402
+
+# the reference's sources, where the oracle recipe (oracle/Makefile print-ref) finds them
+REF = oracle_py.reference_root() or ""
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference sources not present")
+@pytest.mark.skipif(not REF, reason="reference sources not present (oracle/Makefile print-ref)")
 def test_adapter_compiles_against_reference_headers(tmp_path):
     src = tmp_path / "use_adapter.cpp"
     src.write_text('#include "gpu_b200_mpm_solver.h"\n'
@@ -27,7 +30,7 @@ def test_adapter_compiles_against_reference_headers(tmp_path):
     assert r.returncode == 0, r.stderr[-3000:]
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference sources not present")
+@pytest.mark.skipif(not REF, reason="reference sources not present (oracle/Makefile print-ref)")
 def test_sdf_adapter_compiles_against_reference_headers(tmp_path):
     """cressim-mpm_b200/adapter/gpu_b200_sdf_builder.h: the GPU SDF build behind the reference's
     SdfBuilder calls, with SdfDesc / TriangleMesh converted field by field."""

@@ -45,12 +45,19 @@ def _desc(sc, t, stream_shapes):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")
-@pytest.mark.parametrize("kind", ["cube", "quad_slicer"])
+@pytest.mark.parametrize("kind", ["cube", "quad_slicer", "effmass_sphere", "dynamic_sphere"])
 def test_no_alloc_substep_matches_solver_step(kind):
+    """Two calls in a row against two CrB200SolverStep substeps of the same scene: particle state
+    within the parity tolerances, and for the dynamic-shape scenes (the effective-mass contact
+    model and the kinematic one) the coupling force and torque the grid contact accumulates on the
+    shape.  After the two calls the particle positions are also checked against the FP64 oracle
+    directly, so the entry point is pinned independently of the regular solver."""
     import torch
 
+    import oracle_py as op
+
     cb.build_library()
-    sc = scenes.cube_drop() if kind == "cube" else scenes.contact_scene("quad_slicer")
+    sc = scenes.cube_drop() if kind == "cube" else scenes.contact_scene(kind)
     ref = cb.DeviceScene(sc)  # the existing entry points (allocating solver)
     st0 = ref.state()
     dev = ref.device
@@ -85,6 +92,20 @@ def test_no_alloc_substep_matches_solver_step(kind):
         assert float(np.abs(F - a["F"]).max()) <= 1e-4, f"call {call}"
         cscale = max(float(np.abs(a["C"]).max()), 1e-3)
         assert float(np.abs(Cm - a["C"]).max()) <= 1e-3 * cscale, f"call {call}"
+        if kind.endswith("_sphere"):
+            # the dynamic shape's coupling force and torque, accumulated over the calls so far
+            f_ref, q_ref = ref.coupling()
+            for name, got, exp in (("force", shapes["force"], f_ref), ("torque", shapes["torque"], q_ref)):
+                got = got.cpu().numpy()[:, :3]
+                exp = exp[:, :3]
+                scale = max(float(np.abs(exp).max()), 1e-6)
+                assert float(np.abs(got - exp).max()) <= 1e-3 * scale, f"{name}, call {call}"
+    o = op.PortOracle(sc, 64)
+    o.compute_initial_data()
+    o.step(2)
+    x64 = o.state()["x"]
+    x = t["positionMass"][:, :3].cpu().numpy()
+    assert rel_pos_err(x, x64, sc.pos_mass[:, :3], sc.cell_size) <= 1e-4
 
 
 def test_no_alloc_rejects_oversized_grid():
