@@ -412,16 +412,27 @@ def run_ours(args, rank, world, local):
     # per-kernel timing pass (CUDA events around each phase on the solver stream)
     s.set_option(cb.OPT_PHASE_TIMING, 1)
     s.phase_times(reset=True)
+    s.resident_kernel_time(reset=True)
     nprof = min(50, max(10, args.steps // 10))
-    s.step_many(nprof)  # one call, as in the timed region (P2G records carried from G2P after the first)
+    s.step_many(nprof)  # one call, as in the timed region
     phase_ms, nph = s.phase_times(reset=True)
+    fused_ms, fused_n = s.resident_kernel_time(reset=True)
     s.set_option(cb.OPT_PHASE_TIMING, 0)
     per_phase = {name: phase_ms[i] / max(nph, 1) for i, name in enumerate(cb.PHASES)}
     peak, peak_kind = hbm_peak()
+    # algorithmic bytes (200 B per particle and 64 B per touched node per substep) split by kernel:
+    # the fused kernel does one substep's G2P and the next one's P2G, so it reads and writes the
+    # particle state once (200 B) and reads one grid and writes the next (32 B per node)
     alg = {"p2g": 104.0 * n + 16.0 * touched_nodes, "g2p": 96.0 * n + 16.0 * touched_nodes,
-           "grid_update": 32.0 * touched_nodes}
-    dom = max(("p2g", "g2p", "grid_update"), key=lambda k: per_phase[k])
-    achieved = alg[dom] / (per_phase[dom] / 1e3) / 1e9
+           "grid_update": 32.0 * touched_nodes, "g2p2g": 200.0 * n + 32.0 * touched_nodes}
+    if fused_n > 0:
+        # the resident path: the fused G2P -> P2G kernel, timed per launch
+        dom = "g2p2g"
+        per_phase["g2p2g_per_launch"] = fused_ms / fused_n
+        achieved = alg[dom] / (fused_ms / fused_n / 1e3) / 1e9
+    else:
+        dom = max(("p2g", "g2p", "grid_update"), key=lambda k: per_phase[k])
+        achieved = alg[dom] / (per_phase[dom] / 1e3) / 1e9
     substep_bytes = 200.0 * n + 64.0 * touched_nodes
     if scene.solver_type == scenes_mod.SOLVER_PB:
         # PB-MPM step: per iteration read x, v, F, m and read / write C (136 B / particle) and 64 B per

@@ -33,6 +33,7 @@ STATUS_OUT_OF_DOMAIN = 0x4
 OPT_PHASE_TIMING = 3
 OPT_DETERMINISTIC_COUPLING = 4
 OPT_DETERMINISTIC = 5
+OPT_RESIDENT = 6
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 
 
@@ -144,6 +145,7 @@ def lib() -> C.CDLL:
         "CrB200SolverAdvanceAsync": (i, [vp, f, vp, vp, C.POINTER(i)]),
         "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
         "CrB200SolverGetGridStats": (i, [vp, vp]),
+        "CrB200SolverGetResidentKernelTime": (i, [vp, C.POINTER(f), C.POINTER(i), i]),
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
         "CrB200BatchCreate": (i, [i, i, vp, i, i, vp, C.POINTER(vp)]),
         "CrB200SolverAdjointRecord": (i, [vp, i, i, i, vp, vp]),
@@ -402,6 +404,14 @@ class GpuSolver:
         n = C.c_int()
         check(lib().CrB200SolverGetPhaseTimes(self._h, ms, C.byref(n), int(reset)), "phase_times")
         return list(ms), n.value
+
+    def resident_kernel_time(self, reset: bool = True):
+        """(milliseconds, launches) of the resident path's fused G2P -> P2G kernel under phase timing."""
+        ms = C.c_float()
+        n = C.c_int()
+        check(lib().CrB200SolverGetResidentKernelTime(self._h, C.byref(ms), C.byref(n), int(reset)),
+              "resident_kernel_time")
+        return ms.value, n.value
 
     def autotune(self, substeps_per_trial: int = 8):
         """Pick the fastest launch shapes (CrB200SolverAutotune); returns (update CTAs per SM,

@@ -777,6 +777,8 @@ namespace crb200
         const unsigned n = totalParticles();
         if (!n)
             return CRB200_OK;
+        if (int r = residentSyncPlanes()) // F and C of the resident path into the particle-id planes
+            return r;
         k_stateCopy<<<std::min((n + 255) / 256, 2u * (unsigned)strideCtas), 256, 0, stream>>>(
             n, (unsigned)numMaxParticles, false, positionMass, velocity, F, Cm, dst, nullptr, 0u, nullptr, 0u, nullptr);
         CRB_LAUNCHED(1);
@@ -785,6 +787,11 @@ namespace crb200
 
     int Solver::loadState(const unsigned char *src)
     {
+        // the loaded state replaces the resident one (the next resident call re-sorts from it), and
+        // the substeps that follow (the adjoint's replays among them) sort their particles
+        resValid = false;
+        resPlanesStale = false;
+        CRB_CHECK(cudaMemsetAsync(&header->sortSkip, 0, sizeof(unsigned), stream));
         const unsigned n = totalParticles();
         const unsigned nodes = totalBlocks * 64u;
         k_stateCopy<<<std::max(1u, std::min((std::max(n, nodes) + 255) / 256, 2u * (unsigned)strideCtas)), 256, 0, stream>>>(

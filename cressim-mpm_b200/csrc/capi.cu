@@ -250,6 +250,8 @@ extern "C"
             crb200::setLastError("CrB200SolverSetNumActiveParticles: more than numMaxParticles");
             return CRB200_ERR_CAPACITY;
         }
+        if (int rc = s->residentRetire()) // the particle set changes: re-sort at the next resident call
+            return rc;
         s->numActive = n;
         s->configVersion++;
         return CRB200_OK;
@@ -263,6 +265,8 @@ extern "C"
             return bad("CrB200SolverBindParticleData: null pointer");
         if ((reinterpret_cast<uintptr_t>(positionMass) | reinterpret_cast<uintptr_t>(velocity)) & 15u)
             return bad("CrB200SolverBindParticleData: buffers must be 16-byte aligned");
+        if (int rc = s->residentRetire())
+            return rc;
         s->positionMass = reinterpret_cast<float4 *>(positionMass);
         s->velocity = reinterpret_cast<float4 *>(velocity);
         s->configVersion++;
@@ -274,6 +278,8 @@ extern "C"
         SOLVER_OR_FAIL(solver);
         if (!params0 || !type)
             return bad("CrB200SolverBindParticleMaterials: null pointer");
+        if (int rc = s->residentRetire())
+            return rc;
         s->matParams = reinterpret_cast<float4 *>(params0);
         s->matType = type;
         s->configVersion++;
@@ -285,6 +291,8 @@ extern "C"
         SOLVER_OR_FAIL(solver);
         if (!activeMask)
             return bad("CrB200SolverBindActiveMask: null pointer");
+        if (int rc = s->residentRetire())
+            return rc;
         s->activeMask = activeMask;
         s->configVersion++;
         return CRB200_OK;
@@ -370,6 +378,8 @@ extern "C"
         }
         if (n > (unsigned)s->numMaxParticles)
             return bad("CrB200SolverCopyParticleState: n exceeds numMaxParticles");
+        if (int rc = s->residentSyncPlanes())
+            return rc;
         const size_t stride = (size_t)s->numMaxParticles;
         // planes -> per-particle 9 floats: a strided 2D copy per matrix
         if (F)
@@ -410,6 +420,8 @@ extern "C"
         }
         if (n > (unsigned)s->numMaxParticles)
             return bad("CrB200SolverSetParticleState: n exceeds numMaxParticles");
+        if (int rc = s->residentRetire()) // the new state is read from the particle-id planes
+            return rc;
         const size_t stride = (size_t)s->numMaxParticles;
         for (int k = 0; k < 9; ++k)
         {
@@ -446,20 +458,19 @@ extern "C"
             crb200::setLastError("CrB200SolverCopySortState: solver not initialized");
             return CRB200_ERR_NOT_INITIALIZED;
         }
+        // a sort of the current positions, then its products
+        if (keys || sortedIds)
+        {
+            const int r = s->copySortState(keys, sortedIds);
+            if (r != CRB200_OK)
+                return r;
+        }
         crb200::SortHeader h;
         cudaError_t e = cudaMemcpyAsync(&h, s->header, sizeof(h), cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess)
             e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "read sort header");
-        if (keys || sortedIds)
-        {
-            const int r = s->copySortState(keys, h.numSorted ? sortedIds : nullptr);
-            if (r != CRB200_OK)
-                return r;
-        }
-        if (e != cudaSuccess)
-            return crb200::cudaFail(e, "copy sort state");
         if (outNumSortedHost)
             *outNumSortedHost = h.numSorted;
         return CRB200_OK;
@@ -482,6 +493,8 @@ extern "C"
         if (e != cudaSuccess)
             return crb200::cudaFail(e, "read shape flags");
         const unsigned n = s->totalParticles();
+        if (s->resValid && s->numShapes > 0 && (h.shapeFlags & crb200::SF_SLICER))
+            return s->copyCutMasks(masks); // the resident path keeps them in its slots
         if (s->numShapes == 0 || (!s->isBatch() && !(h.shapeFlags & crb200::SF_SLICER)))
             e = cudaMemsetAsync(masks, 0, n * sizeof(unsigned), s->stream); // nothing is cut
         else
@@ -545,6 +558,13 @@ extern "C"
         {
             if (int rc = s->setDeterministic(value != 0))
                 return rc;
+        }
+        else if (option == CRB200_OPT_RESIDENT)
+        {
+            if (value == 0)
+                if (int rc = s->residentRetire())
+                    return rc;
+            s->residentOn = value != 0;
         }
         else
             return bad("CrB200SolverSetOption: unknown option");
@@ -642,6 +662,25 @@ extern "C"
             for (int k = 0; k < CRB200_NUM_PHASES; ++k)
                 s->phaseMs[k] = 0.f;
             s->phaseSteps = 0;
+        }
+        return CRB200_OK;
+    }
+
+    CRB200_API int CrB200SolverGetResidentKernelTime(CrB200SolverHandle solver, float *outMs, int *outLaunches,
+                                                     int reset)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (!outMs || !outLaunches)
+            return bad("CrB200SolverGetResidentKernelTime: null pointer");
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess)
+            return crb200::cudaFail(e, "resident kernel time");
+        *outMs = s->fusedMs;
+        *outLaunches = s->fusedLaunches;
+        if (reset)
+        {
+            s->fusedMs = 0.f;
+            s->fusedLaunches = 0;
         }
         return CRB200_OK;
     }

@@ -60,13 +60,37 @@ namespace crb200
     {
         unsigned numActiveBlocks;
         unsigned numTouchedBlocks;
+        // resident path: particles of the last P2G that left their block (cleared with
+        // numTouchedBlocks and touchedNodes by one memset before every P2G)
+        unsigned resMovers;
+        unsigned touchedNodes;
         unsigned numSorted;
         unsigned status;
         unsigned fp64Fallbacks;
         unsigned shapeFlags;
-        unsigned touchedNodes;
         unsigned recordsValid;   // set by G2P when it binned the particles and wrote the next P2G records
         unsigned pbRecordsValid; // PB-MPM: set by the G2P of an iteration that wrote the next iteration's records
+        unsigned sortSkip;       // the sort kernels of this call return at once (resident path, no re-sort due)
+        unsigned resForce;       // host: re-sort at the next resident call
+        unsigned resFromPlanes;  // host: that re-sort takes F, C, V0 from the particle-id planes
+        unsigned resOutside;     // particles of this call whose stencil left their block's window
+        unsigned matMixed;       // the resident particles' materials differ (else matUniform holds them)
+        unsigned pad;
+        float4 matUniform; // lambda, mu, type (int bits), 0
+    };
+
+    // Resident particle state of the fused single-scene MLS path: slot s holds one particle, slots
+    // grouped by the 4x4x4 grid block (and within it by the cell) the particle sat in at the last
+    // re-sort.
+    struct ResState
+    {
+        float4 *x;          // position, mass
+        float4 *v;          // velocity, initial volume V0
+        float *F, *C;       // 9 planes of `stride` floats, element (r, c) in plane 3c + r
+        const float4 *mat;  // lambda, mu, type (int bits), 0
+        const unsigned *id; // particle id of each slot
+        unsigned *cut;      // slicer cut mask of the position the last P2G used
+        unsigned stride;
     };
 
     class Solver
@@ -243,6 +267,33 @@ namespace crb200
         int detLevel(bool recomputing) const;
         cudaStream_t sideStream = nullptr; // shape gather / cut masks beside the sort chain
         cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
+
+        // Resident path (single-scene MLS-MPM): particle state kept in cell order between substeps,
+        // one fused kernel per substep for G2P of substep k and P2G of substep k + 1, a re-sort only
+        // when particles have left their blocks (resident.cuh).
+        bool residentOn = false;            // CRB200_OPT_RESIDENT
+        bool resValid = false;              // the resident arrays hold the current particle state
+        bool resPlanesStale = false;        // F and C in the particle-id planes are older than the resident ones
+        ResState res{};
+        float4 *resX2 = nullptr, *resV2 = nullptr, *resMat2 = nullptr; // re-sort scratch
+        float *resF2 = nullptr, *resC2 = nullptr;
+        unsigned *resId2 = nullptr, *resSlotOf = nullptr;
+        unsigned *touchedFlag = nullptr;    // per grid block: already in this substep's touched list
+        int resCtas = 0;                    // CTAs of the fused kernel: occupancy x SMs x resMult
+        int resMult = 1;                    // autotuned
+        cudaGraphExec_t resGraph[3] = {nullptr, nullptr, nullptr}; // call start, middle substep, last substep
+        unsigned resGraphVersion = ~0u;
+        int resGraphKernels[3] = {0, 0, 0};
+        float fusedMs = 0.f;                // phase timing: the fused kernel alone
+        int fusedLaunches = 0;
+        bool scratchCoupling = false;       // autotune trials: coupling forces go to scratch
+        bool residentUsable() const;
+        int residentAlloc();
+        int residentStep(int n);
+        int residentPiece(int which);       // 0 call start, 1 middle substep, 2 last substep
+        int residentSyncPlanes();           // F, C back to the particle-id planes
+        int residentRetire();               // planes synced, resident state dropped
+        int copyCutMasks(unsigned *out);
     };
 
     // Grid of one scene (node counts as the reference's solver constructors compute them).

@@ -279,8 +279,9 @@ namespace crb200
                           unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
                           unsigned *__restrict__ cellCount, SortHeader *hdr)
     {
-        if (!Multi && hdr->recordsValid)
-            return; // the previous substep's G2P binned the particles (single scene, MLS)
+        if ((!Multi && hdr->recordsValid) || hdr->sortSkip)
+            return; // the previous substep's G2P binned the particles (single scene, MLS), or the
+                    // resident path keeps its order this call
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
         const unsigned lane = threadIdx.x & 31;
         const unsigned n = Multi ? sc.numParticles : p.numActive;
@@ -314,8 +315,10 @@ namespace crb200
     //    (the block itself or one of its -x/-y/-z neighbours holds particles).
     __global__ void k_scanReduce(StepParams p, SceneTable sc, unsigned totalBlocks,
                                  const unsigned *__restrict__ blockCount, unsigned char *__restrict__ flags,
-                                 uint3 *__restrict__ tileSums)
+                                 uint3 *__restrict__ tileSums, const SortHeader *__restrict__ hdr)
     {
+        if (hdr->sortSkip)
+            return;
         unsigned sum = 0, act = 0, tch = 0;
         const unsigned b0 = blockIdx.x * kScanTile + threadIdx.x * (kScanTile / kScanThreads);
         for (int e = 0; e < kScanTile / kScanThreads; ++e)
@@ -374,6 +377,8 @@ namespace crb200
     // past the buffers.
     __global__ void k_scanTiles(uint3 *__restrict__ tileSums, unsigned numTiles, SortHeader *hdr, unsigned capacity)
     {
+        if (hdr->sortSkip)
+            return;
         __shared__ uint3 carry;
         __shared__ uint3 warpTot[32];
         if (threadIdx.x == 0)
@@ -443,8 +448,10 @@ namespace crb200
     __global__ void k_scanWrite(unsigned totalBlocks, const uint3 *__restrict__ tileOffsets,
                                 unsigned *__restrict__ blockCount, const unsigned char *__restrict__ flags,
                                 unsigned *__restrict__ blockStart, unsigned *__restrict__ activeList,
-                                unsigned *__restrict__ touchedList)
+                                unsigned *__restrict__ touchedList, const SortHeader *__restrict__ hdr)
     {
+        if (hdr->sortSkip)
+            return;
         constexpr int per = kScanTile / kScanThreads;
         const unsigned b0 = blockIdx.x * kScanTile + threadIdx.x * per;
         unsigned cnt[per];
@@ -509,10 +516,10 @@ namespace crb200
     // 4. Scatter (local cell, id) into the block segments.
     __global__ void k_scatter(unsigned numActive, const unsigned *__restrict__ keys, const unsigned *__restrict__ ranks,
                               const unsigned *__restrict__ cellStart, unsigned *__restrict__ sortedIds,
-                              unsigned capacity)
+                              unsigned capacity, const SortHeader *__restrict__ hdr)
     {
         const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= numActive)
+        if (i >= numActive || hdr->sortSkip)
             return;
         const unsigned key = keys[i];
         if (key == kInvalidKey)
@@ -576,6 +583,8 @@ namespace crb200
                                                         const unsigned *__restrict__ blockStart,
                                                         unsigned *__restrict__ cellCount, unsigned *__restrict__ cellStart)
     {
+        if (hdr->sortSkip)
+            return;
         const unsigned lane = threadIdx.x & 31;
         const unsigned nWarps = (gridDim.x * blockDim.x) >> 5;
         const unsigned nAct = hdr->numActiveBlocks;
@@ -669,8 +678,10 @@ namespace crb200
                                                         float4 *__restrict__ detPartials, unsigned *__restrict__ detMask,
                                                         unsigned detMaskWords,
                                                         const float4 *__restrict__ tiles, const float4 *__restrict__ tilesF,
-                                                        const unsigned char *__restrict__ blockFlags)
+                                                        const unsigned char *__restrict__ blockFlags,
+                                                        unsigned *__restrict__ touchedFlag = nullptr)
     {
+        // touchedFlag (resident path): the block's "already listed" flag, cleared as it is consumed
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
         __shared__ float sCouple[Det ? 256 : 1][kDetSlots * 6]; // Det: one row of coupling sums per thread
@@ -701,6 +712,8 @@ namespace crb200
                 if (bi >= nT)
                     break;
                 b = touchedList[bi];
+                if (touchedFlag != nullptr && (threadIdx.x & 63) == 0)
+                    touchedFlag[b] = 0u;
                 const StepParams &p = Multi ? sc.params[sceneOfBlock(sc, b)] : p0;
                 const GridGeom &g = p.g;
                 const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
@@ -1442,6 +1455,27 @@ namespace crb200
                 }
     }
 
+    // Slicer cut mask of one position (checkOnDifferentSides over the 27 stencil nodes,
+    // mpm_rigid_contact.h:401-478): bit a*9 + b*3 + c is set when the particle and stencil node
+    // (a, b, c) lie on different sides of a slicer.
+    __device__ __forceinline__ unsigned cutMaskOf(const GridGeom &g, V3 x, const Stencil &st, const ShapeRec *shp,
+                                                  int numShapes, const SdfPtrs &sdf)
+    {
+        unsigned msk = 0;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c)
+                {
+                    if (!inGrid(g, st.b[0] + a, st.b[1] + b, st.b[2] + c))
+                        continue;
+                    const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
+                                    ex::mul(ex::sub((float)c, st.fx.z), g.dx));
+                    if (differentSides(x, ex::add(x, d), shp, numShapes, sdf, nullptr))
+                        msk |= 1u << (a * 9 + b * 3 + c);
+                }
+        return msk;
+    }
+
     // Cut masks of the current positions (bit a*9 + b*3 + c), for inspection.
     //    Multi: every particle gets a mask (zero in scenes without a slicer).
     template <bool Multi>
@@ -1473,23 +1507,15 @@ namespace crb200
         const V3 x = v3(xm[i]);
         const Stencil st = stencilOf(g, x);
         if (st.finite && p.solverType != CRB200_SOLVER_GPU_STANDARD && mask[i])
-        {
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b)
-                    for (int c = 0; c < 3; ++c)
-                    {
-                        if (!inGrid(g, st.b[0] + a, st.b[1] + b, st.b[2] + c))
-                            continue;
-                        const V3 d = v3(ex::mul(ex::sub((float)a, st.fx.x), g.dx), ex::mul(ex::sub((float)b, st.fx.y), g.dx),
-                                        ex::mul(ex::sub((float)c, st.fx.z), g.dx));
-                        if (differentSides(x, ex::add(x, d), shp, p.numShapes, sdf, nullptr))
-                            msk |= 1u << (a * 9 + b * 3 + c);
-                    }
-        }
+            msk = cutMaskOf(g, x, st, shp, p.numShapes, sdf);
         out[i] = msk;
         }
     }
 
+} // namespace crb200
+#include "resident.cuh"
+namespace crb200
+{
     // The adjoint's tape of one substep's sort products (read back by its reverse substep).
     __global__ void k_tapeSort(unsigned n, unsigned blocks, const unsigned *__restrict__ sortedIds,
                                const unsigned *__restrict__ cellStart, const unsigned *__restrict__ blockStart,
@@ -1722,10 +1748,15 @@ namespace crb200
         for (cudaEvent_t e : phaseEv)
             if (e)
                 cudaEventDestroy(e);
+        for (cudaGraphExec_t &gx : resGraph)
+            if (gx)
+                cudaGraphExecDestroy(gx);
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, cellCount, blockCount, blockStart,
                         activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, cellStart,
                         dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask,
-                        detTiles, detTilesF, detFixedMass};
+                        detTiles, detTilesF, detFixedMass, res.x, res.v, res.F, res.C, const_cast<float4 *>(res.mat),
+                        const_cast<unsigned *>(res.id), res.cut, resSlotOf, resX2, resV2, resMat2, resF2, resC2, resId2,
+                        touchedFlag};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -1919,16 +1950,17 @@ namespace crb200
         }
         unsigned char *flags = blockFlags;
         k_scanReduce<<<numTiles, kScanThreads, 0, stream>>>(p, sc, totalBlocks, blockCount, flags,
-                                                            reinterpret_cast<uint3 *>(tileSums));
+                                                            reinterpret_cast<uint3 *>(tileSums), header);
         k_scanTiles<<<1, 1024, 0, stream>>>(reinterpret_cast<uint3 *>(tileSums), numTiles, header,
                                             (unsigned)numMaxParticles);
         k_scanWrite<<<numTiles, kScanThreads, 0, stream>>>(totalBlocks, reinterpret_cast<const uint3 *>(tileSums),
-                                                           blockCount, flags, blockStart, activeList, touchedList);
+                                                           blockCount, flags, blockStart, activeList, touchedList,
+                                                           header);
         CRB_LAUNCHED(3);
         if (n > 0)
         {
             k_cellStarts<<<cellCtas, 256, 0, stream>>>(header, activeList, blockStart, cellCount, cellStart);
-            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, cellStart, sortedIds, (unsigned)numMaxParticles);
+            k_scatter<<<pg, 128, 0, stream>>>(n, keys, ranks, cellStart, sortedIds, (unsigned)numMaxParticles, header);
             CRB_LAUNCHED(1);
         }
         return CRB200_OK;
@@ -2250,7 +2282,11 @@ namespace crb200
             setLastError("step: solver not initialized");
             return CRB200_ERR_NOT_INITIALIZED;
         }
-        int r = invalidateRecords();
+        if (residentUsable())
+            return residentStep(1);
+        int r = residentRetire(); // back to the particle-id order if the resident path ran before
+        if (r == CRB200_OK)
+            r = invalidateRecords();
         return r != CRB200_OK ? r : launchStep();
     }
 
@@ -2260,7 +2296,7 @@ namespace crb200
     // flag, so that k_bin starts from zero counts.
     int Solver::invalidateRecords()
     {
-        CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, 2 * sizeof(unsigned), stream)); // + pbRecordsValid
+        CRB_CHECK(cudaMemsetAsync(&header->recordsValid, 0, 3 * sizeof(unsigned), stream)); // + pbRecordsValid, sortSkip
         CRB_CHECK(cudaMemsetAsync(blockCount, 0, (totalBlocks + 1) * sizeof(unsigned), stream));
         CRB_CHECK(cudaMemsetAsync(cellCount, 0, (size_t)totalBlocks * 64 * sizeof(unsigned), stream));
         return CRB200_OK;
@@ -2275,7 +2311,11 @@ namespace crb200
         }
         if (n <= 0)
             return CRB200_OK;
-        int rv = invalidateRecords();
+        if (residentUsable())
+            return residentStep(n);
+        int rv = residentRetire(); // back to the particle-id order if the resident path ran before
+        if (rv == CRB200_OK)
+            rv = invalidateRecords();
         if (rv != CRB200_OK)
             return rv;
         if (stream == nullptr || n < 2 || phaseTiming)
@@ -2337,6 +2377,10 @@ namespace crb200
             setLastError("computeInitialData: null index list");
             return CRB200_ERR_INVALID_ARGUMENT;
         }
+        // F = I and V0 of the listed particles go to the particle-id planes: the resident state is
+        // synced first and re-sorted from the planes at the next resident call
+        if (int r = residentRetire())
+            return r;
         const unsigned g = (n + 127) / 128;
         const SceneTable sc = sceneTable();
         if (detP2G && detFixedMass && !isBatch())
@@ -2395,18 +2439,29 @@ namespace crb200
             r = cudaFail(cudaEventCreate(&e0), "autotune event");
         if (r == CRB200_OK)
             r = cudaFail(cudaEventCreate(&e1), "autotune event");
+        // the resident path (single-scene MLS) tunes the grid update and the fused kernel's CTA
+        // multiple; the particle-id path the update, the accumulation and the cell-start kernels
+        const bool resident = residentUsable();
         const bool replay0 = adjReplay;
-        adjReplay = true;
+        if (resident)
+            scratchCoupling = true;
+        else
+            adjReplay = true;
         const int upd[3] = {4, 8, 16}, mul[2] = {1, 2};
         float best = 1e30f;
-        int bestC[3] = {updCtas / std::max(sms, 1), 1, 1};
+        int bestC[3] = {updCtas / std::max(sms, 1), resident ? resMult : 1, 1};
         for (int a = 0; a < 3 && r == CRB200_OK; ++a)
             for (int b = 0; b < 2 && r == CRB200_OK; ++b)
-                for (int c = 0; c < 2 && r == CRB200_OK; ++c)
+                for (int c = 0; c < (resident ? 1 : 2) && r == CRB200_OK; ++c)
                 {
                     updCtas = sms * upd[a];
-                    p2gCtas = baseP2g * mul[b];
-                    cellCtas = baseSort * mul[c];
+                    if (resident)
+                        resMult = mul[b];
+                    else
+                    {
+                        p2gCtas = baseP2g * mul[b];
+                        cellCtas = baseSort * mul[c];
+                    }
                     configVersion++;
                     if ((r = loadState(snap)) != CRB200_OK || (r = stepMany(2)) != CRB200_OK)
                         break; // builds the graph
@@ -2432,9 +2487,15 @@ namespace crb200
                     }
                 }
         adjReplay = replay0;
+        scratchCoupling = false;
         updCtas = sms * bestC[0];
-        p2gCtas = baseP2g * bestC[1];
-        cellCtas = baseSort * bestC[2];
+        if (resident)
+            resMult = bestC[1];
+        else
+        {
+            p2gCtas = baseP2g * bestC[1];
+            cellCtas = baseSort * bestC[2];
+        }
         configVersion++;
         if (r == CRB200_OK)
             r = loadState(snap);
@@ -2454,11 +2515,19 @@ namespace crb200
         return r;
     }
 
+    // The cell keys and the canonical permutation of the current positions: a sort of them now
+    // (the resident path keeps its slots in the order of its last re-sort, which may be older).
     int Solver::copySortState(unsigned *keysOut, unsigned *idsOut)
     {
         const unsigned n = totalParticles();
         if (!n)
             return CRB200_OK;
+        if (int r = residentRetire())
+            return r;
+        if (int r = invalidateRecords())
+            return r;
+        if (int r = sortParticles(params(), solverType == CRB200_SOLVER_GPU_STANDARD))
+            return r;
         if (keysOut)
             CRB_CHECK(cudaMemsetAsync(keysOut, 0xff, n * sizeof(unsigned), stream));
         k_sortKeysOut<<<sortCtas, 64, 0, stream>>>(header, activeList, blockStart, sortedIds, cellStart, keysOut, idsOut);
@@ -2476,4 +2545,5 @@ namespace crb200
     }
 } // namespace crb200
 
+#include "resident_host.cuh"
 #include "adjoint.cuh"

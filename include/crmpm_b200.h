@@ -245,9 +245,10 @@ CRB200_API int CrB200SolverCopyParticleState(CrB200SolverHandle solver, unsigned
 CRB200_API int CrB200SolverSetParticleState(CrB200SolverHandle solver, unsigned int n,
                                             const float *F, const float *C, const float *V0);
 
-/* Sort products of the most recent substep: per-particle block key (uint32, key of an inactive
- * particle is 0xFFFFFFFF) and the canonical permutation (particle ids ordered by key, ties by
- * id) of the `*outNumSorted` binned particles.  Device buffers of numMaxParticles entries. */
+/* The engine's sort of the current positions (the binning of the reference's cell keys,
+ * mls_mpm_algorithm.h:170-175): per-particle block key (uint32, key of an inactive particle is
+ * 0xFFFFFFFF) and the canonical permutation (particle ids ordered by key, ties by id) of the
+ * `*outNumSorted` binned particles.  Device buffers of numMaxParticles entries. */
 CRB200_API int CrB200SolverCopySortState(CrB200SolverHandle solver, unsigned int *keys,
                                          unsigned int *sortedIds, unsigned int *outNumSortedHost);
 
@@ -280,23 +281,44 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
  * Single-scene solvers only; the substeps an adjoint backward pass replays use the ordinary path. */
 #define CRB200_OPT_DETERMINISTIC 5
+/* CRB200_OPT_RESIDENT (off by default; no counterpart in the reference, whose solvers keep the
+ * particles in the caller's order): single-scene MLS-MPM solvers keep their own copy of the
+ * particle state in slots grouped by 4x4x4 grid block and cell, and one fused kernel per substep
+ * does the G2P of one substep and the P2G of the next.  Results are the same as with the option off
+ * up to the order of float sums.  After every step / stepMany call the bound positionMass and
+ * velocity buffers hold the state, as with the option off; edits to them between calls are read at
+ * the next call.  A changed active mask or particle material takes effect at the next call after
+ * BindActiveMask / BindParticleMaterials / SetNumActiveParticles / ComputeInitialData (the
+ * reference's scene makes one of these whenever it changes them).  Deterministic substeps, adjoint
+ * replays and batches use the particle-id-ordered path. */
+#define CRB200_OPT_RESIDENT 6
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the
  * solver stream since the last reset, and the number of substeps they cover.  Phases:
  * 0 shape gather + binning + scan + scatter + cut masks + per-block cell sort, 1 P2G (particle
  * records + cell accumulation), 2 grid update, 3 G2P (PB-MPM: G2P plus the integration kernel).
+ * On the resident path (CRB200_OPT_RESIDENT): 0 the call's start (shape gather, re-sort when due),
+ * 1 the call's first P2G and the fused G2P -> P2G kernels, 2 grid updates, 3 the call's last G2P.
  * Synchronizes the solver stream. */
 #define CRB200_NUM_PHASES 4
 CRB200_API int CrB200SolverGetPhaseTimes(CrB200SolverHandle solver, float outMs[CRB200_NUM_PHASES],
                                          int *outSubsteps, int reset);
+
+/* The fused G2P -> P2G kernel of the resident path (CRB200_OPT_RESIDENT) under phase timing:
+ * CUDA-event milliseconds accumulated over its launches since the last reset, and their number
+ * (no counterpart in the reference).  Synchronizes the solver stream. */
+CRB200_API int CrB200SolverGetResidentKernelTime(CrB200SolverHandle solver, float *outMs, int *outLaunches,
+                                                 int reset);
 
 /* Launch-shape autotuner (no counterpart in the reference): times the candidate CTA counts of
  * the grid update (4, 8 or 16 per SM), the cell accumulation (1x or 2x its occupancy) and the
  * per-cell start computation (4 or 8 per SM) over substepsPerTrial substeps each (0: 8) from the current state, keeps the
  * fastest and restores the state; coupling forces of the trials are not reported.  Writes the
  * choice (update CTAs per SM, accumulation multiple, sort multiple) to outChoiceHost[3] if
- * given.  Needs a non-default solver stream; synchronizes it. */
+ * given.  On the resident path (CRB200_OPT_RESIDENT) the second entry is the fused kernel's
+ * multiple of its occupancy (1x or 2x) and the third is 1.  Needs a non-default solver stream;
+ * synchronizes it. */
 CRB200_API int CrB200SolverAutotune(CrB200SolverHandle solver, int substepsPerTrial, int *outChoiceHost);
 
 /* Grid bookkeeping of the most recent substep: particles binned, active blocks, blocks updated,

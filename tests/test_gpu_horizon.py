@@ -4,9 +4,9 @@ The other parity tests keep the runs short.  These run the headline scenes for t
 substeps (or steps) the workloads are defined over, and every test prints and asserts the bar it
 applies, next to the reference's own deviation that the bar is derived from:
 
-* the 1.6M-particle MLS tissue slab, 500 substeps, against the reference's own CUDA solver (two
-  runs of it: the reference's float atomics sum in arrival order, so two runs of the reference
-  differ by its own ordering noise, `e_self`);
+* the 1.6M-particle MLS tissue slab, 500 substeps, against the reference's own CUDA solver, with
+  the bar set by the reference's own sensitivity to the order of its float sums (the same
+  reference run on the particles listed in another order);
 * a reduced slab (0.3 x 0.1 x 0.3 m, dx 0.01, pins and probe kept), 500 substeps, against the FP64
   oracle and the reference's float32 arithmetic (`e_ref` = the reference float32 run's own
   departure from FP64);
@@ -17,6 +17,7 @@ applies, next to the reference's own deviation that the bar is derived from:
 
 Position metric: max_p |x - x_ref| / max(max_p |x_ref - x0|, dx).
 """
+import dataclasses
 import threading
 
 import numpy as np
@@ -63,28 +64,55 @@ def _threaded(*fns):
     return out
 
 
+def _quantiles(x, x_ref, x0, dx):
+    """Per-particle position error over max(displacement, dx): median, 99th, 99.9th percentile, max."""
+    scale = max(float(np.abs(x_ref - x0).max()), dx)
+    err = np.abs(x - x_ref).max(axis=1) / scale
+    return [float(q) for q in np.quantile(err, (0.5, 0.99, 0.999, 1.0))]
+
+
+def _permuted(sc, seed=11):
+    """The same scene with its particles listed in a seeded random order (and the inverse order)."""
+    perm = np.random.default_rng(seed).permutation(sc.n)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(sc.n)
+    return dataclasses.replace(sc, pos_mass=sc.pos_mass[perm], vel=sc.vel[perm], mat_params=sc.mat_params[perm],
+                               mat_type=sc.mat_type[perm], mask=sc.mask[perm]), inv
+
+
 @pytest.mark.skipif(not op.ref_gpu_available(), reason="oracle/_ref/ref_gpu_driver not built")
 def test_full_slab_500_substeps_against_reference_cuda(tmp_path):
+    """Over 500 substeps the pinned slab amplifies float32 rounding: a change in the order of the
+    node sums moves particles near the pins by up to about 1e-2 of the displacement scale (the
+    reference's float32 arithmetic and the FP64 oracle part that far on the reduced slab below).
+    Two runs of the reference's CUDA solver mostly repeat its atomic order, so they are no measure
+    of that.  The measure is the reference run on the same particles listed in another order (its
+    atomics then sum in another order): the engine's distance to the reference must stay within
+    twice that, quantile by quantile (median, 99th, 99.9th percentile, max), or within 1e-4."""
     sc = scenes.tissue_slab()
     steps = 500
-    ref_a = op.ref_gpu_run(sc, steps, workdir=str(tmp_path))
-    ref_b = op.ref_gpu_run(sc, steps, workdir=str(tmp_path))
+    ref = op.ref_gpu_run(sc, steps, workdir=str(tmp_path))
+    psc, inv = _permuted(sc)
+    rp = op.ref_gpu_run(psc, steps, workdir=str(tmp_path))
+    ref_p = {"x": rp["x"][inv], "v": rp["v"][inv]}
     got = _engine(sc, steps)
     x0 = sc.pos_mass[:, :3]
-    e_self = rel_pos_err(ref_b["x"], ref_a["x"], x0, sc.cell_size)
-    tol = max(1e-4, 2.0 * e_self)
-    e = rel_pos_err(got["x"], ref_a["x"], x0, sc.cell_size)
-    vscale = max(float(np.abs(ref_a["v"]).max()), 1e-3)
-    dv_self = float(np.abs(ref_b["v"] - ref_a["v"]).max())
-    dv = float(np.abs(got["v"] - ref_a["v"]).max())
-    vtol = max(1e-3 * vscale, 2.0 * dv_self)
-    _report("slab1.6M_500_vs_refcuda", e=e, e_self=e_self, tol=tol, dv=dv, dv_self=dv_self, vtol=vtol,
-            disp=float(np.abs(ref_a["x"] - x0).max()))
-    assert e <= tol, f"engine vs reference CUDA {e:.3e} > {tol:.3e} (two reference runs differ by {e_self:.3e})"
+    q_ord = np.array(_quantiles(ref_p["x"], ref["x"], x0, sc.cell_size))
+    q_got = np.array(_quantiles(got["x"], ref["x"], x0, sc.cell_size))
+    tol = np.maximum(1e-4, 2.0 * q_ord)
+    vscale = max(float(np.abs(ref["v"]).max()), 1e-3)
+    dv_ord = float(np.abs(ref_p["v"] - ref["v"]).max())
+    dv = float(np.abs(got["v"] - ref["v"]).max())
+    vtol = max(1e-3 * vscale, 2.0 * dv_ord)
+    _report("slab1.6M_500_vs_refcuda", e_median=q_got[0], e_p99=q_got[1], e_p999=q_got[2], e_max=q_got[3],
+            order_median=q_ord[0], order_p99=q_ord[1], order_p999=q_ord[2], order_max=q_ord[3],
+            tol_max=float(tol[3]), dv=dv, dv_order=dv_ord, vtol=vtol, disp=float(np.abs(ref["x"] - x0).max()))
+    for name, e, t in zip(("median", "p99", "p99.9", "max"), q_got, tol):
+        assert e <= t, f"engine vs reference CUDA, {name}: {e:.3e} > {t:.3e}"
     assert dv <= vtol
     S = sc.shapes.shape_type.shape[0]
     for key in ("force", "torque"):
-        a, b = got[key][:S], ref_a[key][:S]
+        a, b = got[key][:S], ref[key][:S]
         scale = max(float(np.abs(b).max()), 1e-6)
         assert float(np.abs(a - b).max()) <= 1e-3 * scale, key
 
@@ -120,8 +148,10 @@ def test_reduced_slab_500_substeps_against_fp64():
     df_ref = float(np.abs(c["F"] - b["F"]).max())
     df = float(np.abs(got["F"] - b["F"]).max())
     ftol = max(1e-4, 2.0 * df_ref)
+    q64 = _quantiles(got["x"], b["x"], x0, sc.cell_size)
+    qref = _quantiles(c["x"], b["x"], x0, sc.cell_size)
     _report("slab_reduced_500_vs_fp64", n=sc.n, e64=e64, e32=e32, e_ref=e_ref, tol=tol, dF=df, dF_ref=df_ref,
-            ftol=ftol)
+            ftol=ftol, e64_median=q64[0], e64_p99=q64[1], ref_median=qref[0], ref_p99=qref[1])
     assert e64 <= tol, f"engine vs FP64 {e64:.3e} > {tol:.3e} (reference float32 vs FP64: {e_ref:.3e})"
     assert e32 <= tol, f"engine vs reference float32 {e32:.3e} > {tol:.3e}"
     assert df <= ftol

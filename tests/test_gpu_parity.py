@@ -91,14 +91,16 @@ def test_pb_mpm_cube():
 
 
 def test_sort_keys_and_permutation_bitexact():
+    """CrB200SolverCopySortState sorts the current positions: cell keys and the canonical
+    permutation (by key, ties by particle id) bit for bit against numpy."""
     sc = scenes.cube_drop()
     g = _gpu(sc)
     for _ in range(3):
-        g.sync()
-        x_before = g.pos[: sc.n, :3].cpu().numpy()
         g.step(1, graph=False)
+        g.sync()
+        x_now = g.pos[: sc.n, :3].cpu().numpy()
         keys, ids = g.sort_state()
-        exp = block_keys(sc, x_before)
+        exp = block_keys(sc, x_now)
         np.testing.assert_array_equal(keys, exp)
         np.testing.assert_array_equal(ids, canonical_permutation(exp, sc.mask.astype(bool)))
         g.step(40)
