@@ -14,9 +14,8 @@
 //      cell, cell), the rank from a shared counter per cell; 192 threads, one per (cell, x-slab of
 //      the 3x3x3 stencil), add their cell's records into registers and add those sums into a
 //      shared 8x8x8 output window, warp by warp (no atomics);
-//   4. particles that moved out of the block (or beyond a cell's kResRanks) are added to the
-//      output window with shared-memory atomics, those that left the window (or the grid) with
-//      global vector atomics;
+//   4. particles that moved out of the block, left the window (or the grid) or come beyond a
+//      cell's kResRanks are added with global vector atomics (fire-and-forget reductions);
 //   5. the output window goes to the accumulation grid with one float4 vector atomic per node that
 //      received mass, and the grid blocks it touched are appended to the touched-block list the
 //      grid update walks.
@@ -87,40 +86,31 @@ namespace crb200
                 }
     }
 
-    // One particle's record added to the shared output window at window offset (rx, ry, rz) of its
-    // base cell, with shared-memory atomics (particles that left their block, overflow of a cell).
-    __device__ __forceinline__ void resScatterWindow(float (*out)[kOutCh], int rx, int ry, int rz, const float *rec,
-                                                     unsigned msk)
+    // One particle's record added straight to the accumulation grid with one float4 vector
+    // reduction per in-grid node not cut off by a slicer (a crowded cell's particles beyond
+    // kResRanks, and particles that left their block but not its window).  Fire-and-forget
+    // reductions keep the warp moving; the caller has the blocks listed for the grid update.
+    __device__ __forceinline__ void resScatterRed(const GridGeom &g, const Stencil &st, const float *rec, unsigned msk,
+                                                  float4 *__restrict__ gridA)
     {
         float w[3][3];
-        weights(v3(rec[13], rec[14], rec[15]), w);
+        weights(st.fx, w);
         const V3 u = v3(rec[0], rec[1], rec[2]);
         const V3 a0 = v3(rec[4], rec[5], rec[6]), a1 = v3(rec[7], rec[8], rec[9]), a2 = v3(rec[10], rec[11], rec[12]);
-        const float m = rec[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
-        {
-            const V3 ui = u + a0 * (float)i;
 #pragma unroll
             for (int j = 0; j < 3; ++j)
-            {
-                const V3 uij = ui + a1 * (float)j;
-                const float wij = w[i][0] * w[j][1];
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
                 {
-                    if ((msk >> (i * 9 + j * 3 + k)) & 1u)
+                    const int ni = st.b[0] + i, nj = st.b[1] + j, nk = st.b[2] + k;
+                    if (!inGrid(g, ni, nj, nk) || ((msk >> (i * 9 + j * 3 + k)) & 1u))
                         continue;
-                    const float wt = wij * w[k][2];
-                    const V3 val = uij + a2 * (float)k;
-                    const int t = (rx + i) + 8 * (ry + j) + kOutZ * (rz + k);
-                    atomicAdd(&out[0][t], val.x * wt);
-                    atomicAdd(&out[1][t], val.y * wt);
-                    atomicAdd(&out[2][t], val.z * wt);
-                    atomicAdd(&out[3][t], m * wt);
+                    const float wt = (w[i][0] * w[j][1]) * w[k][2];
+                    const V3 val = ((u + a0 * (float)i) + a1 * (float)j) + a2 * (float)k;
+                    atomicAdd(&gridA[nodeAddr(g, ni, nj, nk)], make_float4(val.x * wt, val.y * wt, val.z * wt, rec[3] * wt));
                 }
-            }
-        }
     }
 
     // The fused substep kernel.  DoG2P: G2P of the current substep from the grid velocities.
@@ -129,7 +119,7 @@ namespace crb200
     // buffers instead of the resident ones.  Without DoG2P (the first substep of a call) positions
     // and velocities come from the caller's buffers, so edits made between calls are honoured.
     template <bool DoG2P, bool DoP2G, bool Export>
-    __global__ void __maxnreg__(112)
+    __global__ void __launch_bounds__(kResThreads, 3)
         k_g2p2g(const __grid_constant__ StepParams p, SortHeader *hdr, const unsigned *__restrict__ activeList,
                 const unsigned *__restrict__ blockStart, ResState rs, float4 *callerX, float4 *callerV,
                 const float4 *__restrict__ gridV, float4 *__restrict__ gridA, unsigned *__restrict__ touchedFlag,
@@ -385,8 +375,28 @@ namespace crb200
                     if (rank >= (unsigned)kResRanks)
                     {
                         const int rx = sn.b[0] - ox, ry = sn.b[1] - oy, rz = sn.b[2] - oz;
-                        if (inside && rx >= 0 && rx <= 5 && ry >= 0 && ry <= 5 && rz >= 0 && rz <= 5)
-                            resScatterWindow(S.out, rx, ry, rz, rec, msk);
+                        if (inBlock)
+                        {
+                            // a crowded cell: the cell's first kResRanks records cover the same nodes,
+                            // so the window flush lists their blocks
+                            resScatterRed(g, sn, rec, 0u, gridA);
+                        }
+                        else if (inside && rx >= 0 && rx <= 5 && ry >= 0 && ry <= 5 && rz >= 0 && rz <= 5)
+                        {
+                            // left the block, not the window: the blocks of its stencil (within the
+                            // 3x3x3 neighbourhood of this block) are listed by the flush
+                            resScatterRed(g, sn, rec, msk, gridA);
+                            unsigned bits = 0u;
+                            const int l0[3] = {(sn.b[0] >> 2) - bx + 1, (sn.b[1] >> 2) - by + 1, (sn.b[2] >> 2) - bz + 1};
+                            const int l1[3] = {(min(sn.b[0] + 2, g.n.x - 1) >> 2) - bx + 1,
+                                               (min(sn.b[1] + 2, g.n.y - 1) >> 2) - by + 1,
+                                               (min(sn.b[2] + 2, g.n.z - 1) >> 2) - bz + 1};
+                            for (int zz = l0[2]; zz <= l1[2]; ++zz)
+                                for (int yy = l0[1]; yy <= l1[1]; ++yy)
+                                    for (int xx = l0[0]; xx <= l1[0]; ++xx)
+                                        bits |= 1u << (xx + 3 * yy + 9 * zz);
+                            atomicOr(&S.touchedBits, bits);
+                        }
                         else if (sn.finite)
                         {
                             // left the window, or a stencil across the grid boundary (the record is
@@ -519,11 +529,11 @@ namespace crb200
 
     // Whether this call re-sorts the resident slots: on request of the host (first call, changed
     // particle set or state) or when the previous call left particles outside their block's window
-    // or more than one in eight outside its block.  The sort kernels return at once otherwise.
+    // or more than one in 64 outside its block.  The sort kernels return at once otherwise.
     __global__ void k_resDecide(SortHeader *hdr)
     {
         const bool want = hdr->resForce != 0u || hdr->resOutside != 0u ||
-                          (unsigned long long)hdr->resMovers * 8ull > (unsigned long long)hdr->numSorted;
+                          (unsigned long long)hdr->resMovers * 64ull > (unsigned long long)hdr->numSorted;
         hdr->sortSkip = want ? 0u : 1u;
         hdr->resOutside = 0u;
         if (want)
