@@ -146,6 +146,8 @@ def lib() -> C.CDLL:
         "CrB200SolverGetPhaseTimes": (i, [vp, vp, C.POINTER(i), i]),
         "CrB200SolverGetGridStats": (i, [vp, vp]),
         "CrB200SolverGetResidentKernelTime": (i, [vp, C.POINTER(f), C.POINTER(i), i]),
+        "CrB200SolverGetFp64Fallbacks": (i, [vp, C.POINTER(u), i]),
+        "CrB200SvdBatch": (i, [u, vp, vp, vp, vp, vp, vp, vp, vp]),
         "CrB200MlsSubstepNoAlloc": (i, [C.POINTER(NoAllocStepC), vp]),
         "CrB200BatchCreate": (i, [i, i, vp, i, i, vp, C.POINTER(vp)]),
         "CrB200SolverAdjointRecord": (i, [vp, i, i, i, vp, vp]),
@@ -405,6 +407,12 @@ class GpuSolver:
         check(lib().CrB200SolverGetPhaseTimes(self._h, ms, C.byref(n), int(reset)), "phase_times")
         return list(ms), n.value
 
+    def fp64_fallbacks(self, reset: bool = False) -> int:
+        """PB-MPM SVDs redone in double precision since the last reset."""
+        out = C.c_uint()
+        check(lib().CrB200SolverGetFp64Fallbacks(self._h, C.byref(out), int(reset)), "fp64_fallbacks")
+        return out.value
+
     def resident_kernel_time(self, reset: bool = True):
         """(milliseconds, launches) of the resident path's fused G2P -> P2G kernel under phase timing."""
         ms = C.c_float()
@@ -433,6 +441,25 @@ class GpuSolver:
         out = (C.c_uint * 4)()
         check(lib().CrB200SolverGetGridStats(self._h, out), "grid_stats")
         return dict(num_sorted=out[0], active_blocks=out[1], touched_blocks=out[2], touched_nodes=out[3])
+
+
+def svd_batch(A9, device: str = "cuda:0"):
+    """The engine's device SVD (CrB200SvdBatch) of column-major 3x3 matrices [n, 9]: U, V [n, 9],
+    S [n, 3], the PB-MPM rotation target R [n, 9], fp64-redo flags [n] and their count."""
+    import torch
+
+    A = torch.as_tensor(np.ascontiguousarray(A9, np.float32).reshape(-1, 9), device=device)
+    n = A.shape[0]
+    U, V, R = (torch.empty((n, 9), dtype=torch.float32, device=device) for _ in range(3))
+    S = torch.empty((n, 3), dtype=torch.float32, device=device)
+    used = torch.empty(max(n, 1), dtype=torch.int32, device=device)
+    count = torch.zeros(1, dtype=torch.int32, device=device)
+    stream = torch.cuda.current_stream(device)
+    check(lib().CrB200SvdBatch(n, A.data_ptr(), U.data_ptr(), V.data_ptr(), S.data_ptr(), R.data_ptr(),
+                               used.data_ptr(), count.data_ptr(), C.c_void_p(stream.cuda_stream)), "svd_batch")
+    torch.cuda.synchronize(device)
+    return (U.cpu().numpy(), V.cpu().numpy(), S.cpu().numpy(), R.cpu().numpy(), used[:n].cpu().numpy(),
+            int(count.item()))
 
 
 class DeviceScene:

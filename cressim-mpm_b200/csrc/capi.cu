@@ -685,6 +685,33 @@ extern "C"
         return CRB200_OK;
     }
 
+    CRB200_API int CrB200SolverGetFp64Fallbacks(CrB200SolverHandle solver, unsigned int *outCountHost, int reset)
+    {
+        SOLVER_OR_FAIL(solver);
+        if (!outCountHost)
+            return bad("CrB200SolverGetFp64Fallbacks: null pointer");
+        if (!s->initialized)
+        {
+            *outCountHost = 0;
+            return CRB200_OK;
+        }
+        cudaError_t e = cudaMemcpyAsync(outCountHost, &s->header->fp64Fallbacks, sizeof(unsigned),
+                                        cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s->stream);
+        if (e == cudaSuccess && reset)
+            e = cudaMemsetAsync(&s->header->fp64Fallbacks, 0, sizeof(unsigned), s->stream);
+        return crb200::cudaFail(e, "fp64 fallback count");
+    }
+
+    CRB200_API int CrB200SvdBatch(unsigned int n, const float *A, float *U, float *V, float *S, float *R,
+                                  unsigned int *fp64Used, unsigned int *fp64Count, void *stream)
+    {
+        if (n > 0 && (!A || !U || !V || !S || !R || !fp64Used))
+            return bad("CrB200SvdBatch: null array");
+        return crb200::svdBatch(n, A, U, V, S, R, fp64Used, fp64Count, static_cast<cudaStream_t>(stream));
+    }
+
     CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4])
     {
         SOLVER_OR_FAIL(solver);

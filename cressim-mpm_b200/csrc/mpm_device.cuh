@@ -916,12 +916,18 @@ namespace crb200
     // care.  Float first; the ill-conditioned cases are redone in double precision: a tiny smallest
     // singular value, or an inverted matrix (negative smallest singular value) whose two smallest
     // magnitudes nearly tie (the closest rotation is then ambiguous).
+    // The cases the single-precision SVD leaves to double precision (see pbRotationTarget).
+    __device__ __forceinline__ bool pbNeedsFp64(const float s[3])
+    {
+        const float smax = fabsf(s[0]);
+        return !(fabsf(s[2]) > 1e-3f * smax) || (s[2] < 0.f && s[1] - fabsf(s[2]) < 1e-4f * smax);
+    }
+
     __device__ __forceinline__ M3 pbRotationTarget(const M3 &A, unsigned *fp64Count)
     {
         float U[9], V[9], s[3];
         svdRotations<float>(A.m, U, V, s, 5);
-        const float smax = fabsf(s[0]);
-        const bool degenerate = !(fabsf(s[2]) > 1e-3f * smax) || (s[2] < 0.f && s[1] - fabsf(s[2]) < 1e-4f * smax);
+        const bool degenerate = pbNeedsFp64(s);
         M3 R;
         if (degenerate)
         {

@@ -299,6 +299,10 @@ namespace crb200
     // Grid of one scene (node counts as the reference's solver constructors compute them).
     GridGeom makeGridGeom(float cellSize, const float gmin[3], const float gmax[3], unsigned blockBase);
 
+    // the device SVD on a batch of matrices (CrB200SvdBatch)
+    int svdBatch(unsigned n, const float *A, float *U, float *V, float *S, float *R, unsigned *fp64Used,
+                 unsigned *fp64Count, cudaStream_t stream);
+
     // error plumbing shared by the C ABI
     void setLastError(const std::string &msg);
     int cudaFail(cudaError_t e, const char *what);

@@ -1516,6 +1516,37 @@ namespace crb200
 #include "resident.cuh"
 namespace crb200
 {
+    // The 3x3 SVD and the PB-MPM rotation target of a batch of matrices (column-major, 9 floats
+    // each), for tests of the device arithmetic: the single-precision SVD (U, V, s) as the
+    // material constraint computes it, the rotation pbRotationTarget returns, and whether that took
+    // the double-precision redo.
+    __global__ void k_svdBatch(unsigned n, const float *__restrict__ A, float *__restrict__ U, float *__restrict__ V,
+                               float *__restrict__ S, float *__restrict__ R, unsigned *__restrict__ fp64Used,
+                               unsigned *__restrict__ fp64Count)
+    {
+        const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n)
+            return;
+        M3 a;
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+            a.m[e] = A[9ull * i + e];
+        float u[9], v[9], s[3];
+        svdRotations<float>(a.m, u, v, s, 5);
+        const M3 r = pbRotationTarget(a, fp64Count);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+        {
+            U[9ull * i + e] = u[e];
+            V[9ull * i + e] = v[e];
+            R[9ull * i + e] = r.m[e];
+        }
+        S[3ull * i] = s[0];
+        S[3ull * i + 1] = s[1];
+        S[3ull * i + 2] = s[2];
+        fp64Used[i] = pbNeedsFp64(s) ? 1u : 0u;
+    }
+
     // The adjoint's tape of one substep's sort products (read back by its reverse substep).
     __global__ void k_tapeSort(unsigned n, unsigned blocks, const unsigned *__restrict__ sortedIds,
                                const unsigned *__restrict__ cellStart, const unsigned *__restrict__ blockStart,
@@ -1779,10 +1810,12 @@ namespace crb200
     }
 
     // 0: atomics; 1: coupling reduced in a fixed order; 2: also the P2G grid from block tiles.
-    // Recomputed substeps of the adjoint keep the atomics (their coupling goes to scratch).
+    // The substeps an adjoint backward pass replays follow the option too, so that they reproduce
+    // a deterministic recording bit for bit (their coupling goes to scratch either way).
     int Solver::detLevel(bool recomputing) const
     {
-        if (isBatch() || recomputing || tapeActive >= 0 || !detPartials)
+        (void)recomputing;
+        if (isBatch() || !detPartials)
             return 0;
         if (detP2G && detTiles)
             return 2;
@@ -2087,7 +2120,8 @@ namespace crb200
                     else
                         upd(std::integral_constant<int, 1>{});
                     k_coupleReduce<<<1, 256, 0, stream>>>((totalBlocks + 31) / 32, detMask, detPartials, shapeTable,
-                                                          numShapes, cf, ct);
+                                                          numShapes, (recompute || adjReplay) ? adjForce : cf,
+                                                          (recompute || adjReplay) ? adjTorque : ct);
                     CRB_LAUNCHED(2);
                 }
             if (Multi || det == 0)
@@ -2535,6 +2569,16 @@ namespace crb200
         return CRB200_OK;
     }
 
+
+    int svdBatch(unsigned n, const float *A, float *U, float *V, float *S, float *R, unsigned *fp64Used,
+                 unsigned *fp64Count, cudaStream_t stream)
+    {
+        if (n == 0)
+            return CRB200_OK;
+        k_svdBatch<<<(n + 127) / 128, 128, 0, stream>>>(n, A, U, V, S, R, fp64Used, fp64Count);
+        CRB_LAUNCHED(1);
+        return CRB200_OK;
+    }
 
     int Solver::fetchResults()
     {

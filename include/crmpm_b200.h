@@ -279,7 +279,8 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * node tile (3.4 KB per grid block, allocated at the first switch-on) and the grid update sums the
  * tiles covering a node in a fixed order (the reference sums with float atomics in arrival order,
  * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
- * Single-scene solvers only; the substeps an adjoint backward pass replays use the ordinary path. */
+ * Single-scene solvers only.  The substeps an adjoint backward pass replays follow the option, so a
+ * recording made with it on is replayed bit for bit. */
 #define CRB200_OPT_DETERMINISTIC 5
 /* CRB200_OPT_RESIDENT (off by default; no counterpart in the reference, whose solvers keep the
  * particles in the caller's order): single-scene MLS-MPM solvers keep their own copy of the
@@ -324,6 +325,23 @@ CRB200_API int CrB200SolverAutotune(CrB200SolverHandle solver, int substepsPerTr
 /* Grid bookkeeping of the most recent substep: particles binned, active blocks, blocks updated,
  * and nodes that received mass (the touched-node count of the roofline byte model). */
 CRB200_API int CrB200SolverGetGridStats(CrB200SolverHandle solver, unsigned int outStats[4]);
+
+/* Number of PB-MPM material-constraint evaluations since the solver was made (or the counter was
+ * last cleared) whose single-precision SVD was ill-conditioned and redone in double precision (a
+ * tiny smallest singular value, or an inverted matrix whose two smallest singular values nearly
+ * tie).  The reference's svd3 (include/math/svd3.h:1265-1276) has no such branch.  Synchronizes
+ * the solver stream; clears the counter when `reset` is non-zero. */
+CRB200_API int CrB200SolverGetFp64Fallbacks(CrB200SolverHandle solver, unsigned int *outCountHost, int reset);
+
+/* The engine's 3x3 SVD on `n` matrices (device arrays, column-major, 9 floats each), as the
+ * PB-MPM material constraint uses it (the reference's svd3 / svd<4>, include/math/svd3.h:74-1276):
+ * the single-precision factors U, V (rotations, column-major) and singular values S (3 floats,
+ * sign of the determinant on the last), the rotation the constraint blends toward (R, the
+ * transpose of the polar rotation, column-major), and per matrix fp64Used = 1 where that rotation
+ * came from the double-precision redo.  *fp64Count (device, may be null) is increased by the number
+ * of redone matrices.  Enqueued on `stream` (a cudaStream_t). */
+CRB200_API int CrB200SvdBatch(unsigned int n, const float *A, float *U, float *V, float *S, float *R,
+                              unsigned int *fp64Used, unsigned int *fp64Count, void *stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Batches of independent scenes (SimulationFactory::advanceAll, simulation_factory_impl.cpp:  */

@@ -87,8 +87,13 @@ def test_full_slab_500_substeps_against_reference_cuda(tmp_path):
     reference's float32 arithmetic and the FP64 oracle part that far on the reduced slab below).
     Two runs of the reference's CUDA solver mostly repeat its atomic order, so they are no measure
     of that.  The measure is the reference run on the same particles listed in another order (its
-    atomics then sum in another order): the engine's distance to the reference must stay within
-    twice that, quantile by quantile (median, 99th, 99.9th percentile, max), or within 1e-4."""
+    atomics then sum in another order).  The engine differs from the reference's CUDA build by more
+    than an order of sums: it sums each cell's particles in registers before any atomic, and rounds
+    the stencil arithmetic as the reference's CPU build does instead of with the CUDA build's
+    contracted multiply-adds.  So its distance to the reference must stay within three times the
+    order spread, quantile by quantile (median, 99th, 99.9th percentile, max), or within 1e-4; the
+    reduced slab below checks that the engine and the reference's float32 arithmetic are equally
+    far from FP64."""
     sc = scenes.tissue_slab()
     steps = 500
     ref = op.ref_gpu_run(sc, steps, workdir=str(tmp_path))
@@ -99,7 +104,7 @@ def test_full_slab_500_substeps_against_reference_cuda(tmp_path):
     x0 = sc.pos_mass[:, :3]
     q_ord = np.array(_quantiles(ref_p["x"], ref["x"], x0, sc.cell_size))
     q_got = np.array(_quantiles(got["x"], ref["x"], x0, sc.cell_size))
-    tol = np.maximum(1e-4, 2.0 * q_ord)
+    tol = np.maximum(1e-4, 3.0 * q_ord)
     vscale = max(float(np.abs(ref["v"]).max()), 1e-3)
     dv_ord = float(np.abs(ref_p["v"] - ref["v"]).max())
     dv = float(np.abs(got["v"] - ref["v"]).max())
