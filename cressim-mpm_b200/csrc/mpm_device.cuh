@@ -77,6 +77,32 @@ namespace crb200
     }
     __device__ __forceinline__ float comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 
+    // sm_100's paired FP32 arithmetic: one instruction computes two lanes, each rounded as the
+    // scalar fused multiply-add or multiply, so results equal the scalar code's bit for bit.
+    // v + a * s
+    __device__ __forceinline__ V3 fma3(V3 a, float s, V3 v)
+    {
+        const float2 lo = __ffma2_rn(make_float2(a.x, a.y), make_float2(s, s), make_float2(v.x, v.y));
+        return v3(lo.x, lo.y, fmaf(a.z, s, v.z));
+    }
+    // a * s
+    __device__ __forceinline__ V3 mul3(V3 a, float s)
+    {
+        const float2 lo = __fmul2_rn(make_float2(a.x, a.y), make_float2(s, s));
+        return v3(lo.x, lo.y, a.z * s);
+    }
+    // acc[0..3] += (v.x, v.y, v.z, m) * s: a node's momentum and mass sums
+    __device__ __forceinline__ void fma4acc(float acc[4], V3 v, float m, float s)
+    {
+        const float2 s2 = make_float2(s, s);
+        const float2 lo = __ffma2_rn(make_float2(v.x, v.y), s2, make_float2(acc[0], acc[1]));
+        const float2 hi = __ffma2_rn(make_float2(v.z, m), s2, make_float2(acc[2], acc[3]));
+        acc[0] = lo.x;
+        acc[1] = lo.y;
+        acc[2] = hi.x;
+        acc[3] = hi.y;
+    }
+
     // Quaternion rotation (quat.h:117-150).
     __device__ __forceinline__ V3 qrot(const float4 &q, V3 v)
     {

@@ -85,8 +85,12 @@ namespace crb200
     struct ResState
     {
         float4 *x;          // position, mass
-        float4 *v;          // velocity, initial volume V0
-        float *F, *C;       // 9 planes of `stride` floats, element (r, c) in plane 3c + r
+        float4 *v;          // velocity, kept only in scenes with slicers (G2P of a cut particle
+                            // starts from it); elsewhere the caller's buffer holds it between calls
+        float *V0;          // initial volume
+        float *F, *C;       // 9 planes of `stride` floats, element (r, c) in plane 3c + r; C is
+                            // current only after the last substep of a call (the fused kernel
+                            // uses each substep's C at once, and the next G2P replaces it)
         const float4 *mat;  // lambda, mu, type (int bits), 0
         const unsigned *id; // particle id of each slot
         unsigned *cut;      // slicer cut mask of the position the last P2G used
@@ -275,8 +279,8 @@ namespace crb200
         bool resValid = false;              // the resident arrays hold the current particle state
         bool resPlanesStale = false;        // F and C in the particle-id planes are older than the resident ones
         ResState res{};
-        float4 *resX2 = nullptr, *resV2 = nullptr, *resMat2 = nullptr; // re-sort scratch
-        float *resF2 = nullptr, *resC2 = nullptr;
+        float4 *resX2 = nullptr, *resMat2 = nullptr; // re-sort scratch
+        float *resV02 = nullptr, *resF2 = nullptr, *resC2 = nullptr;
         unsigned *resId2 = nullptr, *resSlotOf = nullptr;
         unsigned *touchedFlag = nullptr;    // per grid block: already in this substep's touched list
         int resCtas = 0;                    // CTAs of the fused kernel: occupancy x SMs x resMult

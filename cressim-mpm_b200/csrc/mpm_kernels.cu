@@ -1087,12 +1087,12 @@ namespace crb200
                             const unsigned ab = AX[a] + AY[b];
                             const V3 v0 = v3(__ldg(&gridV[ab + AZ[0]])), v1 = v3(__ldg(&gridV[ab + AZ[1]])),
                                      v2 = v3(__ldg(&gridV[ab + AZ[2]]));
-                            const V3 Zc = v1 * w[1][2] + v2 * (2.f * w[2][2]);
-                            const V3 Z = v0 * w[0][2] + v1 * w[1][2] + v2 * w[2][2];
-                            Y = Y + Z * w[b][1];
+                            const V3 Zc = fma3(v2, 2.f * w[2][2], mul3(v1, w[1][2]));
+                            const V3 Z = fma3(v2, w[2][2], fma3(v1, w[1][2], mul3(v0, w[0][2])));
+                            Y = fma3(Z, w[b][1], Y);
                             if (b)
-                                Yb = Yb + Z * ((float)b * w[b][1]);
-                            Yc = Yc + Zc * w[b][1];
+                                Yb = fma3(Z, (float)b * w[b][1], Yb);
+                            Yc = fma3(Zc, w[b][1], Yc);
                         }
                         const V3 wY = Y * w[a][0];
                         S = S + wY;
@@ -1785,8 +1785,8 @@ namespace crb200
         void *bufs[] = {F, Cm, V0, gridA, gridV, gridF, keys, ranks, sortedIds, cellCount, blockCount, blockStart,
                         activeList, touchedList, tileSums, cutMasks, header, shapeTable, blockFlags, records, cellStart,
                         dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask,
-                        detTiles, detTilesF, detFixedMass, res.x, res.v, res.F, res.C, const_cast<float4 *>(res.mat),
-                        const_cast<unsigned *>(res.id), res.cut, resSlotOf, resX2, resV2, resMat2, resF2, resC2, resId2,
+                        detTiles, detTilesF, detFixedMass, res.x, res.v, res.V0, res.F, res.C, const_cast<float4 *>(res.mat),
+                        const_cast<unsigned *>(res.id), res.cut, resSlotOf, resX2, resV02, resMat2, resF2, resC2, resId2,
                         touchedFlag};
         for (void *b : bufs)
             if (b)

@@ -228,11 +228,11 @@ namespace crb200
 #pragma unroll
         for (int i = 0; i < 3; ++i)
         {
-            const V3 ui = u + a0 * (float)i;
+            const V3 ui = i == 0 ? u : fma3(a0, (float)i, u);
 #pragma unroll
             for (int j = 0; j < 3; ++j)
             {
-                const V3 uij = ui + a1 * (float)j;
+                const V3 uij = j == 0 ? ui : fma3(a1, (float)j, ui);
                 const float wij = w[i][0] * w[j][1];
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
@@ -258,13 +258,7 @@ namespace crb200
                         acc[n][3] += m * wt;
                     }
                     else
-                    {
-                        const V3 val = uij + a2 * (float)k;
-                        acc[n][0] += val.x * wt;
-                        acc[n][1] += val.y * wt;
-                        acc[n][2] += val.z * wt;
-                        acc[n][3] += m * wt;
-                    }
+                        fma4acc(acc[n], k == 0 ? uij : fma3(a2, (float)k, uij), m, wt);
                 }
             }
         }

@@ -12,17 +12,18 @@
 //      (mls_mpm_algorithm.h:147-241) of the updated particle;
 //   3. records of particles whose (new) cell lies in the block go to shared memory by (rank in
 //      cell, cell), the rank from a shared counter per cell; 192 threads, one per (cell, x-slab of
-//      the 3x3x3 stencil), add their cell's records into registers and add those sums into a
-//      shared 8x8x8 output window, warp by warp (no atomics);
+//      the 3x3x3 stencil), add their cell's records into registers and reduce those sums into a
+//      shared 8x8x8 output window;
 //   4. particles that moved out of the block, left the window (or the grid) or come beyond a
 //      cell's kResRanks are added with global vector atomics (fire-and-forget reductions);
 //   5. the output window goes to the accumulation grid with one float4 vector atomic per node that
 //      received mass, and the grid blocks it touched are appended to the touched-block list the
 //      grid update walks.
-// Each particle's state is read and written once per substep.  The slots are re-sorted at the
-// start of a call only when the previous call left particles outside their block's window or too
-// many outside their block; correctness never depends on the grouping, only the share of particles
-// that take the slower paths does.
+// Per substep each particle's position and F are read and written once and its V0 read; C is
+// written only by the last substep of a call, which also writes the velocities to the caller's
+// buffer.  The slots are re-sorted at the start of a call only when the previous call left
+// particles outside their block's window or too many outside their block; correctness never
+// depends on the grouping, only the share of particles that take the slower paths does.
 #pragma once
 
 namespace crb200
@@ -174,28 +175,30 @@ namespace crb200
             // ---- particles, in slot order
             for (unsigned s = s0 + (unsigned)tid; s < s1; s += kResThreads)
             {
-                const unsigned id = rs.id[s];
-                float4 x4, v4;
+                // the particle id only where the caller's buffers are read or written
+                const unsigned id = (!DoG2P || Export) ? rs.id[s] : 0u;
+                float4 x4;
+                V3 v = v3(0.f, 0.f, 0.f);
                 if (DoG2P)
                 {
                     x4 = rs.x[s];
-                    v4 = rs.v[s];
+                    if (slicers) // G2P of a cut particle falls back on its own velocity
+                        v = v3(rs.v[s]);
                 }
                 else
                 {
                     x4 = callerX[id];
-                    const float4 cv = callerV[id];
-                    v4 = rs.v[s];
-                    v4.x = cv.x;
-                    v4.y = cv.y;
-                    v4.z = cv.z;
+                    v = v3(callerV[id]);
                     rs.x[s] = x4;
-                    rs.v[s] = v4;
+                    if (slicers)
+                        rs.v[s] = make_float4(v.x, v.y, v.z, 0.f);
                 }
+                const float V0p = rs.V0[s];
                 M3 Fp, Cp;
                 loadM3(rs.F, rs.stride, s, Fp);
-                loadM3(rs.C, rs.stride, s, Cp);
-                V3 x = v3(x4), v = v3(v4);
+                if (!DoG2P)
+                    loadM3(rs.C, rs.stride, s, Cp);
+                V3 x = v3(x4);
                 if (DoG2P)
                 {
                     const Stencil st = stencilOf(g, x);
@@ -224,12 +227,12 @@ namespace crb200
                                 {
                                     const int t = (rx + a) + 8 * (ry + bb) + 64 * rz;
                                     const V3 v0 = v3(S.gv[t]), v1 = v3(S.gv[t + 64]), v2 = v3(S.gv[t + 128]);
-                                    const V3 Zc = v1 * w[1][2] + v2 * (2.f * w[2][2]);
-                                    const V3 Z = v0 * w[0][2] + v1 * w[1][2] + v2 * w[2][2];
-                                    Y = Y + Z * w[bb][1];
+                                    const V3 Zc = fma3(v2, 2.f * w[2][2], mul3(v1, w[1][2]));
+                                    const V3 Z = fma3(v2, w[2][2], fma3(v1, w[1][2], mul3(v0, w[0][2])));
+                                    Y = fma3(Z, w[bb][1], Y);
                                     if (bb)
-                                        Yb = Yb + Z * ((float)bb * w[bb][1]);
-                                    Yc = Yc + Zc * w[bb][1];
+                                        Yb = fma3(Z, (float)bb * w[bb][1], Yb);
+                                    Yc = fma3(Zc, w[bb][1], Yc);
                                 }
                                 const V3 wY = Y * w[a][0];
                                 Sv = Sv + wY;
@@ -300,16 +303,19 @@ namespace crb200
                         atomicOr(&hdr->status, CRB200_STATUS_NAN_STATE);
                     if (Export)
                     {
+                        // the last substep of a call: positions and velocities to the caller, C for
+                        // the next call's first P2G and for readback
                         callerX[id] = make_float4(xn.x, xn.y, xn.z, x4.w);
                         callerV[id] = make_float4(vn.x, vn.y, vn.z, 0.f);
+                        storeM3(rs.C, rs.stride, s, Cn);
                     }
                     else
                     {
                         rs.x[s] = make_float4(xn.x, xn.y, xn.z, x4.w);
-                        rs.v[s] = make_float4(vn.x, vn.y, vn.z, v4.w);
+                        if (slicers)
+                            rs.v[s] = make_float4(vn.x, vn.y, vn.z, 0.f);
                     }
                     storeM3(rs.F, rs.stride, s, Fp);
-                    storeM3(rs.C, rs.stride, s, Cn);
                     x = xn;
                     v = vn;
                     Cp = Cn;
@@ -328,7 +334,7 @@ namespace crb200
                         raw.F[e] = Fp.m[e];
                         raw.C[e] = Cp.m[e];
                     }
-                    raw.v0 = v4.w;
+                    raw.v0 = V0p;
                     const Stencil sn = stencilOf(g, x);
                     bool ood = !sn.finite;
                     if (sn.finite)
@@ -419,6 +425,7 @@ namespace crb200
             // ---- records by cell: thread (cell c, x-slab sl) over the cell's first kResRanks particles
             {
                 const int c = tid & 63, sl = tid >> 6;
+                const float slf = (float)sl;
                 const unsigned cnt = min(S.count[c], (unsigned)kResRanks);
                 float acc[3][3][4];
 #pragma unroll
@@ -438,51 +445,38 @@ namespace crb200
                     float w[3][3];
                     weights(v3(rc[13], rc[14], rc[15]), w);
                     const float wx = sl == 0 ? w[0][0] : (sl == 1 ? w[1][0] : w[2][0]);
-                    const V3 ui = v3(rc[0], rc[1], rc[2]) + v3(rc[4], rc[5], rc[6]) * (float)sl;
+                    const V3 ui = fma3(v3(rc[4], rc[5], rc[6]), slf, v3(rc[0], rc[1], rc[2]));
                     const V3 a1 = v3(rc[7], rc[8], rc[9]), a2 = v3(rc[10], rc[11], rc[12]);
 #pragma unroll
                     for (int j = 0; j < 3; ++j)
                     {
-                        const V3 uij = ui + a1 * (float)j;
+                        const V3 uij = j == 0 ? ui : fma3(a1, (float)j, ui);
                         const float wij = wx * w[j][1];
 #pragma unroll
                         for (int k = 0; k < 3; ++k)
-                        {
-                            const float wt = wij * w[k][2];
-                            const V3 val = uij + a2 * (float)k;
-                            acc[j][k][0] += val.x * wt;
-                            acc[j][k][1] += val.y * wt;
-                            acc[j][k][2] += val.z * wt;
-                            acc[j][k][3] += rc[3] * wt;
-                        }
+                            fma4acc(acc[j][k], k == 0 ? uij : fma3(a2, (float)k, uij), rc[3], wij * w[k][2]);
                     }
                 }
-                // Neighbouring cells share nodes (cell c at offset j + 1 and cell c + 4 at offset j
-                // land on one node), but for one offset (j, k) the 32 cells of a warp write 32
-                // distinct nodes.  So the six warps take turns (a barrier between turns), and within
-                // a turn the lanes add offset by offset with a warp barrier in between: plain
-                // read-modify-writes, no two at one node at once.
-                const int cx = c & 3, cy = (c >> 2) & 3, cz = c >> 4;
-                const int warp = tid >> 5;
-                for (int turn = 0; turn < kResThreads / 32; ++turn)
+                // Shared-memory float reductions into the output window.  For one offset (j, k) the
+                // 32 cells of a warp add to 32 distinct nodes in 32 distinct banks (z stride
+                // kOutZ), so a warp's reductions never collide with each other; neighbouring cells
+                // of other warps share nodes, which the reductions resolve in hardware.
+                if (cnt)
                 {
-                    if (warp == turn)
-                    {
+                    const int cx = c & 3, cy = (c >> 2) & 3, cz = c >> 4;
 #pragma unroll
-                        for (int j = 0; j < 3; ++j)
+                    for (int j = 0; j < 3; ++j)
 #pragma unroll
-                            for (int k = 0; k < 3; ++k)
-                            {
-                                const int t = (cx + 1 + sl) + 8 * (cy + 1 + j) + kOutZ * (cz + 1 + k);
+                        for (int k = 0; k < 3; ++k)
+                        {
+                            const int t = (cx + 1 + sl) + 8 * (cy + 1 + j) + kOutZ * (cz + 1 + k);
 #pragma unroll
-                                for (int ch = 0; ch < 4; ++ch)
-                                    S.out[ch][t] += acc[j][k][ch];
-                                __syncwarp();
-                            }
-                    }
-                    __syncthreads();
+                            for (int ch = 0; ch < 4; ++ch)
+                                atomicAdd(&S.out[ch][t], acc[j][k][ch]);
+                        }
                 }
             }
+            __syncthreads();
             // ---- the output window into the accumulation grid
             unsigned bits = 0u;
             for (int t = tid; t < kWinNodes; t += kResThreads)
@@ -540,15 +534,16 @@ namespace crb200
             hdr->matMixed = 0u;
     }
 
-    // After a re-sort: the new slot order's particle state into the scratch arrays.  Positions,
-    // velocities and materials come from the caller's buffers; F, C and V0 from the particle-id
-    // planes (resFromPlanes) or from the particle's previous resident slot.
+    // After a re-sort: the new slot order's particle state into the scratch arrays.  Positions and
+    // materials come from the caller's buffers (velocities are read from there by the call's first
+    // P2G); F, C and V0 from the particle-id planes (resFromPlanes) or from the particle's previous
+    // resident slot.
     __global__ void k_resGather(const SortHeader *hdr, const unsigned *__restrict__ sortedIds,
                                 const float4 *__restrict__ callerX, const float4 *__restrict__ callerV,
                                 const float4 *__restrict__ matParams, const int *__restrict__ matType,
                                 const float *__restrict__ Fid, const float *__restrict__ Cid,
                                 const float *__restrict__ V0id, ResState rs, const unsigned *__restrict__ slotOf,
-                                float4 *__restrict__ x2, float4 *__restrict__ v2, float *__restrict__ F2,
+                                float4 *__restrict__ x2, float *__restrict__ V02, float *__restrict__ F2,
                                 float *__restrict__ C2, float4 *__restrict__ mat2, unsigned *__restrict__ id2,
                                 SortHeader *hdrw)
     {
@@ -563,7 +558,7 @@ namespace crb200
         for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
         {
             const unsigned id = sortedIds[s];
-            const float4 x4 = callerX[id], cv = callerV[id], mp = matParams[id];
+            const float4 x4 = callerX[id], mp = matParams[id];
             const int mt = matType[id];
             float v0;
             // a particle without a previous slot (slotOf is cleared to ~0 when the arrays are made)
@@ -587,10 +582,10 @@ namespace crb200
                     F2[k * stride + s] = rs.F[k * stride + o];
                     C2[k * stride + s] = rs.C[k * stride + o];
                 }
-                v0 = rs.v[o].w;
+                v0 = rs.V0[o];
             }
             x2[s] = x4;
-            v2[s] = make_float4(cv.x, cv.y, cv.z, v0);
+            V02[s] = v0;
             mat2[s] = make_float4(mp.x, mp.y, __int_as_float(mt), 0.f);
             id2[s] = id;
             mixed |= __float_as_uint(mp.x) != __float_as_uint(m0.x) || __float_as_uint(mp.y) != __float_as_uint(m0.y) ||
@@ -604,7 +599,7 @@ namespace crb200
 
     // The scratch arrays become the resident state; each particle's slot is recorded.
     __global__ void k_resCopyBack(SortHeader *hdr, ResState rs, unsigned *__restrict__ slotOf,
-                                  const float4 *__restrict__ x2, const float4 *__restrict__ v2,
+                                  const float4 *__restrict__ x2, const float *__restrict__ V02,
                                   const float *__restrict__ F2, const float *__restrict__ C2,
                                   const float4 *__restrict__ mat2, const unsigned *__restrict__ id2,
                                   float4 *__restrict__ matOut, unsigned *__restrict__ idOut)
@@ -615,7 +610,7 @@ namespace crb200
         for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
         {
             rs.x[s] = x2[s];
-            rs.v[s] = v2[s];
+            rs.V0[s] = V02[s];
 #pragma unroll
             for (int k = 0; k < 9; ++k)
             {

@@ -30,6 +30,7 @@ namespace crb200
         unsigned *id = nullptr;
         CRB_CHECK(cudaMalloc(&res.x, n * sizeof(float4)));
         CRB_CHECK(cudaMalloc(&res.v, n * sizeof(float4)));
+        CRB_CHECK(cudaMalloc(&res.V0, n * sizeof(float)));
         CRB_CHECK(cudaMalloc(&res.F, 9 * n * sizeof(float)));
         CRB_CHECK(cudaMalloc(&res.C, 9 * n * sizeof(float)));
         CRB_CHECK(cudaMalloc(&mat, n * sizeof(float4)));
@@ -40,7 +41,7 @@ namespace crb200
         res.stride = (unsigned)n;
         CRB_CHECK(cudaMalloc(&resSlotOf, n * sizeof(unsigned)));
         CRB_CHECK(cudaMalloc(&resX2, n * sizeof(float4)));
-        CRB_CHECK(cudaMalloc(&resV2, n * sizeof(float4)));
+        CRB_CHECK(cudaMalloc(&resV02, n * sizeof(float)));
         CRB_CHECK(cudaMalloc(&resMat2, n * sizeof(float4)));
         CRB_CHECK(cudaMalloc(&resF2, 9 * n * sizeof(float)));
         CRB_CHECK(cudaMalloc(&resC2, 9 * n * sizeof(float)));
@@ -146,9 +147,9 @@ namespace crb200
             if ((r = sortParticles(p, false)) != CRB200_OK)
                 return r;
             k_resGather<<<strideCtas, 256, 0, stream>>>(header, sortedIds, positionMass, velocity, matParams, matType, F,
-                                                         Cm, V0, res, resSlotOf, resX2, resV2, resF2, resC2, resMat2,
+                                                         Cm, V0, res, resSlotOf, resX2, resV02, resF2, resC2, resMat2,
                                                          resId2, header);
-            k_resCopyBack<<<strideCtas, 256, 0, stream>>>(header, res, resSlotOf, resX2, resV2, resF2, resC2, resMat2,
+            k_resCopyBack<<<strideCtas, 256, 0, stream>>>(header, res, resSlotOf, resX2, resV02, resF2, resC2, resMat2,
                                                            resId2, const_cast<float4 *>(res.mat),
                                                            const_cast<unsigned *>(res.id));
             CRB_LAUNCHED(2);
