@@ -373,6 +373,8 @@ def run_ours(args, rank, world, local):
         ds.compute_initial_data()
     s = ds.solver
     stream = ds.stream
+    if args.resident:
+        s.set_option(cb.OPT_RESIDENT, 1)
     # warm-up (graph capture happens on the first replay), then the launch-shape autotuner
     ds.step(max(args.warmup, 3))
     tuned = (0, 0, 0) if args.quick else s.autotune(10)  # --quick: short runs for profiler launch lists
@@ -533,6 +535,7 @@ def run_ours(args, rank, world, local):
         "data": "synthetic (seeded jittered particles)",
         "config": {"workload": desc, "particles": n, "grid": list(s.grid_dims()), "dt": scene.dt,
                    "substeps_per_step": 1, "parallelism": f"replicas x{world}",
+                   "path": "resident cell-ordered (CRB200_OPT_RESIDENT)" if args.resident else "particle-id order",
                    "l2": "inputs larger than L2 (particle state ~350 MB)", "touched_nodes": touched_nodes,
                    "autotuned_launch": {"update_ctas_per_sm": tuned[0], "accumulate_x": tuned[1], "sort_x": tuned[2]}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -899,6 +902,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--deterministic", action="store_true",
                     help="single-scene workloads: run the timed substeps with CRB200_OPT_DETERMINISTIC on")
+    ap.add_argument("--resident", action="store_true",
+                    help="single-scene MLS workloads: the resident cell-ordered path (CRB200_OPT_RESIDENT)")
     ap.add_argument("--quick", action="store_true",
                     help="timed region only (no phase pass, e2e or CPU baseline): for profiler launch lists")
     ap.add_argument("--no-extras", action="store_true",
