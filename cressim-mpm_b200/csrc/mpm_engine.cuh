@@ -201,6 +201,10 @@ namespace crb200
         cudaGraphExec_t graph = nullptr;
         unsigned graphVersion = ~0u;
         int graphKernels = 0;
+        // The substeps of a call but its last: their G2P leaves the velocity and C to the P2G record
+        // it writes for the next substep (leanG2P is set while this graph is captured).
+        cudaGraphExec_t graphLean = nullptr;
+        bool leanG2P = false;
 
         StepParams params() const;
         SceneTable sceneTable() const;

@@ -997,12 +997,15 @@ namespace crb200
                                                  unsigned *__restrict__ ranks, unsigned *__restrict__ blockCount,
                                                  unsigned *__restrict__ cellCount,
                                                  const unsigned long long *__restrict__ blockShapeMask,
-                                                 float4 *xo, float4 *vo, float *Fo, float *Co)
+                                                 float4 *xo, float4 *vo, float *Fo, float *Co, bool lean)
     {
         // Modes 0 and 2 write the updated state to xo, vo, Fo, Co: the input arrays themselves in an
         // ordinary substep, the next tape slot in the adjoint's replay (which keeps its input).
         // Inputs and outputs may therefore alias, so none of xm, vel, F, Cm, xo, vo, Fo, Co is
         // declared __restrict__; each thread reads its own particle before it writes it.
+        // lean (MLS, a substep of a call but its last): a particle whose next P2G record is written
+        // here does not write its velocity and C, which only that record carries forward; the
+        // call's last substep writes them for the caller and the next call.
         // One scene: all or nothing (no slicer in the scene).  Batch: per particle, for the scenes
         // without a slicer (k_bin / k_record skip exactly those particles in the next substep).
         if (Mode == 1 && blockIdx.x == 0 && threadIdx.x == 0)
@@ -1205,14 +1208,16 @@ namespace crb200
         for (int e = 0; e < 9; ++e)
             Mu.m[e] = ((e % 4) == 0 ? 1.f : 0.f) + Cn.m[e] * p.dt;
         Fp = matmul(Mu, Fp);
+        const bool carried = kRecords && writeRecords && !(Multi && (sc.flags[si] & SF_SLICER));
         xo[i] = make_float4(xn.x, xn.y, xn.z, x4.w);
-        vo[i] = make_float4(vn.x, vn.y, vn.z, 0.f);
+        if (!(lean && carried))
+            vo[i] = make_float4(vn.x, vn.y, vn.z, 0.f);
         storeM3(Fo, stride, i, Fp);
-        if (Mode == 0)
+        if (Mode == 0 && !(lean && carried))
             storeM3(Co, stride, i, Cn);
         if (!(isfinite(xn.x) && isfinite(xn.y) && isfinite(xn.z) && isfinite(vn.x) && isfinite(vn.y) && isfinite(vn.z)))
             atomicOr(status, CRB200_STATUS_NAN_STATE);
-        if (kRecords && writeRecords && !(Multi && (sc.flags[si] & SF_SLICER)))
+        if (carried)
         {
             RawParticle raw;
             raw.x4 = make_float4(xn.x, xn.y, xn.z, x4.w);
@@ -1776,6 +1781,8 @@ namespace crb200
     {
         if (graph)
             cudaGraphExecDestroy(graph);
+        if (graphLean)
+            cudaGraphExecDestroy(graphLean);
         for (cudaEvent_t e : phaseEv)
             if (e)
                 cudaEventDestroy(e);
@@ -2149,7 +2156,8 @@ namespace crb200
                                                     (M == 0 || (M == 1 && pbRecords)) ? records : nullptr, gridA, header, keys, ranks,
                                                     blockCount, cellCount, blockShapeMask,
                                                     outX ? outX : positionMass, outX ? outV : velocity,
-                                                    outX ? outF : F, outX ? outC : Cm);
+                                                    outX ? outF : F, outX ? outC : Cm,
+                                                    M == 0 && !Multi && leanG2P && outX == nullptr);
             CRB_LAUNCHED(1);
             return CRB200_OK;
         };
@@ -2364,35 +2372,44 @@ namespace crb200
         }
         if (graph == nullptr || graphVersion != configVersion)
         {
-            if (graph)
+            for (cudaGraphExec_t *gx : {&graph, &graphLean})
+                if (*gx)
+                {
+                    cudaGraphExecDestroy(*gx);
+                    *gx = nullptr;
+                }
+            // the full substep, and (single-scene MLS) the lean one for all but a call's last
+            const bool withLean = !isBatch() && solverType == CRB200_SOLVER_GPU_MLS;
+            for (int k = 0; k < (withLean ? 2 : 1); ++k)
             {
-                cudaGraphExecDestroy(graph);
-                graph = nullptr;
+                const uint64_t before = launchCount();
+                leanG2P = k == 1;
+                CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                int r = launchStep();
+                cudaGraph_t g = nullptr;
+                cudaError_t e = cudaStreamEndCapture(stream, &g);
+                leanG2P = false;
+                const uint64_t captured = launchCount() - before;
+                noteLaunches((uint64_t)0 - captured); // captured, not yet executed
+                if (r != CRB200_OK)
+                {
+                    if (g)
+                        cudaGraphDestroy(g);
+                    return r;
+                }
+                if (e != cudaSuccess)
+                    return cudaFail(e, "cudaStreamEndCapture");
+                e = cudaGraphInstantiate(k == 1 ? &graphLean : &graph, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess)
+                    return cudaFail(e, "cudaGraphInstantiate");
+                graphKernels = (int)captured;
             }
-            const uint64_t before = launchCount();
-            CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-            int r = launchStep();
-            cudaGraph_t g = nullptr;
-            cudaError_t e = cudaStreamEndCapture(stream, &g);
-            const uint64_t captured = launchCount() - before;
-            noteLaunches((uint64_t)0 - captured); // captured, not yet executed
-            if (r != CRB200_OK)
-            {
-                if (g)
-                    cudaGraphDestroy(g);
-                return r;
-            }
-            if (e != cudaSuccess)
-                return cudaFail(e, "cudaStreamEndCapture");
-            e = cudaGraphInstantiate(&graph, g, 0);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess)
-                return cudaFail(e, "cudaGraphInstantiate");
-            graphKernels = (int)captured;
             graphVersion = configVersion;
         }
-        for (int i = 0; i < n; ++i)
-            CRB_CHECK(cudaGraphLaunch(graph, stream));
+        for (int i = 0; i < n - 1; ++i)
+            CRB_CHECK(cudaGraphLaunch(graphLean ? graphLean : graph, stream));
+        CRB_CHECK(cudaGraphLaunch(graph, stream));
         noteLaunches((uint64_t)graphKernels * (uint64_t)n);
         return CRB200_OK;
     }
