@@ -41,6 +41,9 @@ namespace crmpm
             const float mn[3] = {mGridBound.minimum.x(), mGridBound.minimum.y(), mGridBound.minimum.z()};
             const float mx[3] = {mGridBound.maximum.x(), mGridBound.maximum.y(), mGridBound.maximum.z()};
             check(CrB200SolverCreate(mType, mNumMaxParticles, mCellSize, mn, mx, mCudaStream, &mHandle));
+            // inactive particles of standard MPM as GpuStandardMpmSolver treats them
+            if (mType == static_cast<int>(MpmSolverType::eGpuStandardMpmSolver))
+                check(CrB200SolverSetOption(mHandle, CRB200_OPT_STANDARD_GPU_SEMANTICS, 1));
             check(CrB200SolverBindParticleData(mHandle, reinterpret_cast<CrB200Float4 *>(mParticleData->positionMass),
                                                reinterpret_cast<CrB200Float4 *>(mParticleData->velocity)));
             check(CrB200SolverBindParticleMaterials(mHandle,

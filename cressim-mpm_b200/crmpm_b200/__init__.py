@@ -34,6 +34,7 @@ OPT_PHASE_TIMING = 3
 OPT_DETERMINISTIC_COUPLING = 4
 OPT_DETERMINISTIC = 5
 OPT_RESIDENT = 6
+OPT_STANDARD_GPU_SEMANTICS = 7
 PHASES = ("sort", "p2g", "grid_update", "g2p")
 
 

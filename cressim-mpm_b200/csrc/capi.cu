@@ -566,6 +566,11 @@ extern "C"
                     return rc;
             s->residentOn = value != 0;
         }
+        else if (option == CRB200_OPT_STANDARD_GPU_SEMANTICS)
+        {
+            if (int rc = s->setStdGpuSemantics(value != 0))
+                return rc;
+        }
         else
             return bad("CrB200SolverSetOption: unknown option");
         s->configVersion++;

@@ -280,6 +280,11 @@ namespace crb200
         // one fused kernel per substep for G2P of substep k and P2G of substep k + 1, a re-sort only
         // when particles have left their blocks (resident.cuh).
         bool residentOn = false;            // CRB200_OPT_RESIDENT
+        // CRB200_OPT_STANDARD_GPU_SEMANTICS: standard MPM as the reference's GPU solver runs it
+        // (G2P ignores the active mask, computeInitialData takes particles 0..n-1)
+        bool stdGpuSemantics = false;
+        unsigned char *onesMask = nullptr;  // numMaxParticles ones
+        unsigned *iotaIds = nullptr;        // 0, 1, ..., numMaxParticles - 1
         bool resValid = false;              // the resident arrays hold the current particle state
         bool resPlanesStale = false;        // F and C in the particle-id planes are older than the resident ones
         ResState res{};
@@ -298,6 +303,7 @@ namespace crb200
         bool residentUsable() const;
         int residentAlloc();
         int residentStep(int n);
+        int setStdGpuSemantics(bool on);
         int residentPiece(int which);       // 0 call start, 1 middle substep, 2 last substep
         int residentSyncPlanes();           // F, C back to the particle-id planes
         int residentRetire();               // planes synced, resident state dropped

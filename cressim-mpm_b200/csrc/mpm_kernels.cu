@@ -1794,7 +1794,7 @@ namespace crb200
                         dParams, dParticleScene, dSceneFlags, blockShapeMask, detPartials, detMask,
                         detTiles, detTilesF, detFixedMass, res.x, res.v, res.V0, res.F, res.C, const_cast<float4 *>(res.mat),
                         const_cast<unsigned *>(res.id), res.cut, resSlotOf, resX2, resV02, resMat2, resF2, resC2, resId2,
-                        touchedFlag};
+                        touchedFlag, onesMask, iotaIds};
         for (void *b : bufs)
             if (b)
                 cudaFree(b);
@@ -2151,7 +2151,8 @@ namespace crb200
             constexpr int M = decltype(mode)::value;
             if (!pg)
                 return CRB200_OK;
-            k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, activeMask, F, Cm, stride, shapeTable,
+            const unsigned char *g2pMask = (M == 2 && stdGpuSemantics && onesMask) ? onesMask : activeMask;
+            k_g2p<M, Multi><<<pg, 128, 0, stream>>>(p, sc, positionMass, velocity, g2pMask, F, Cm, stride, shapeTable,
                                                     sp, gridV, cutMasks, &header->status, matParams, matType, V0,
                                                     (M == 0 || (M == 1 && pbRecords)) ? records : nullptr, gridA, header, keys, ranks,
                                                     blockCount, cellCount, blockShapeMask,
@@ -2414,6 +2415,33 @@ namespace crb200
         return CRB200_OK;
     }
 
+    __global__ void k_iota(unsigned n, unsigned *__restrict__ out)
+    {
+        for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            out[i] = i;
+    }
+
+    // The reference's GPU standard-MPM solver reads the active mask in P2G only and ignores the
+    // index list of computeInitialData, initialising particles 0..n-1
+    // (gpu_standard_mpm_solver.cu:210-212, 280-282, 357-359); its CPU solver honours both.  The
+    // engine follows the CPU solver unless this is on.
+    int Solver::setStdGpuSemantics(bool on)
+    {
+        if (on && !onesMask)
+        {
+            const size_t n = (size_t)numMaxParticles;
+            CRB_CHECK(cudaMalloc(&onesMask, n));
+            CRB_CHECK(cudaMalloc(&iotaIds, n * sizeof(unsigned)));
+            CRB_CHECK(cudaMemsetAsync(onesMask, 1, n, stream));
+            k_iota<<<strideCtas, 256, 0, stream>>>((unsigned)n, iotaIds);
+            CRB_LAUNCHED(1);
+        }
+        if (stdGpuSemantics != on)
+            configVersion++;
+        stdGpuSemantics = on;
+        return CRB200_OK;
+    }
+
     int Solver::computeInitialData(unsigned n, const unsigned *indices)
     {
         if (!initialized)
@@ -2432,6 +2460,15 @@ namespace crb200
         // synced first and re-sorted from the planes at the next resident call
         if (int r = residentRetire())
             return r;
+        if (stdGpuSemantics && solverType == CRB200_SOLVER_GPU_STANDARD && !isBatch())
+        {
+            if (n > (unsigned)numMaxParticles)
+            {
+                setLastError("computeInitialData: more particles than numMaxParticles");
+                return CRB200_ERR_INVALID_ARGUMENT;
+            }
+            indices = iotaIds; // particles 0..n-1, whatever the list
+        }
         const unsigned g = (n + 127) / 128;
         const SceneTable sc = sceneTable();
         if (detP2G && detFixedMass && !isBatch())

@@ -293,6 +293,13 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * reference's scene makes one of these whenever it changes them).  Deterministic substeps, adjoint
  * replays and batches use the particle-id-ordered path. */
 #define CRB200_OPT_RESIDENT 6
+/* CRB200_OPT_STANDARD_GPU_SEMANTICS (standard MPM; off by default): inactive particles as the
+ * reference's GPU solver treats them.  That solver reads the active mask in P2G only, so particles
+ * below the active count that the mask switches off still move with the grid in G2P, and its
+ * computeInitialData initialises particles 0..n-1 whatever the index list
+ * (gpu_standard_mpm_solver.cu:210-212, 280-282, 357-359).  Off, the engine follows the reference's
+ * CPU solver, which honours both.  The drop-in adapter for eGpuStandardMpmSolver turns it on. */
+#define CRB200_OPT_STANDARD_GPU_SEMANTICS 7
 CRB200_API int CrB200SolverSetOption(CrB200SolverHandle solver, int option, int value);
 
 /* Phase timing (CRB200_OPT_PHASE_TIMING on): CUDA-event milliseconds accumulated per phase on the

@@ -59,6 +59,9 @@ def test_factory_cube_through_the_c_api(scene, frames, tol, tmp_path):
     got = _run("b200", scene, frames, tmp_path)
     assert float(np.abs(ref["x"][:, :3] - ref["x0"][:, :3]).max()) > 1e-3, "the cube did not move"
     _compare(got, ref, tol, scene)
+    # a small scene shows the host cost a frame adds (10 substeps, the adapter's C-ABI calls)
+    print(f"FACTORY {scene} frame ms (10 substeps): reference {np.median(ref['times'][1:]) * 1e3:.3f}, "
+          f"drop-in {np.median(got['times'][1:]) * 1e3:.3f}")
 
 
 @pytest.mark.skipif(not built, reason="oracle/_ref/factory not built (make -C oracle ref-factory)")

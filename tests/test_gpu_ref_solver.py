@@ -122,3 +122,32 @@ def test_reference_cuda_solver_pb_cutting(tmp_path):
     err = np.abs(got["x"] - ref["x"]).max(axis=1) / scale
     assert float(err.max()) <= 2e-3
     assert float(np.quantile(err, 0.99)) <= 1e-4, f"99th percentile {np.quantile(err, 0.99):.3e}"
+
+
+def test_standard_mpm_inactive_particles_as_the_reference_gpu_solver(tmp_path):
+    """The reference's GPU standard-MPM solver reads the active mask in P2G only and initialises
+    particles 0..n-1 whatever the index list (gpu_standard_mpm_solver.cu:210-212, 280-282, 357-359);
+    its CPU solver honours both.  With the last 15 % of a cube's particles switched off by the mask,
+    the engine with CRB200_OPT_STANDARD_GPU_SEMANTICS (what the drop-in adapter sets for
+    eGpuStandardMpmSolver) gives the reference CUDA run's positions for every particle, the
+    switched-off ones falling with the grid; without it they stay where they are, as in the
+    reference's CPU solver."""
+    sc = scenes.cube_drop(solver=scenes.SOLVER_STANDARD, dt=1e-4)
+    k = int(sc.n * 0.85)
+    sc.mask[k:] = 0
+    steps = 100
+    ref = op.ref_gpu_run(sc, steps, workdir=str(tmp_path))
+    idx = np.nonzero(sc.mask)[0]
+    out = {}
+    for on in (True, False):
+        cb.build_library()
+        g = cb.DeviceScene(sc, compute_initial=False)
+        g.solver.set_option(cb.OPT_STANDARD_GPU_SEMANTICS, 1 if on else 0)
+        g.compute_initial_data(idx)
+        g.step(steps)
+        out[on] = g.state()
+    x0 = sc.pos_mass[:, :3]
+    assert float(np.abs(ref["x"][k:] - x0[k:]).max()) > 1e-3, "the reference left the switched-off particles"
+    e = rel_pos_err(out[True]["x"], ref["x"], x0, sc.cell_size)
+    assert e <= 1e-4, f"engine with the GPU solver's semantics vs reference CUDA: {e:.3e}"
+    np.testing.assert_array_equal(out[False]["x"][k:], x0[k:])
