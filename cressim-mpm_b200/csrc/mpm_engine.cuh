@@ -205,6 +205,10 @@ namespace crb200
         // it writes for the next substep (leanG2P is set while this graph is captured).
         cudaGraphExec_t graphLean = nullptr;
         bool leanG2P = false;
+        // step(): the record invalidation and one substep
+        cudaGraphExec_t graphSingle = nullptr;
+        unsigned graphSingleVersion = ~0u;
+        int graphSingleKernels = 0;
 
         StepParams params() const;
         SceneTable sceneTable() const;

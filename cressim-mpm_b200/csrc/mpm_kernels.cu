@@ -1783,6 +1783,8 @@ namespace crb200
             cudaGraphExecDestroy(graph);
         if (graphLean)
             cudaGraphExecDestroy(graphLean);
+        if (graphSingle)
+            cudaGraphExecDestroy(graphSingle);
         for (cudaEvent_t e : phaseEv)
             if (e)
                 cudaEventDestroy(e);
@@ -2328,9 +2330,50 @@ namespace crb200
         if (residentUsable())
             return residentStep(1);
         int r = residentRetire(); // back to the particle-id order if the resident path ran before
-        if (r == CRB200_OK)
+        if (r != CRB200_OK)
+            return r;
+        if (stream == nullptr || phaseTiming)
+        {
             r = invalidateRecords();
-        return r != CRB200_OK ? r : launchStep();
+            return r != CRB200_OK ? r : launchStep();
+        }
+        // A scene steps one substep per call (scene_impl.cpp:314-317): the record invalidation and
+        // the substep are replayed from one captured graph, one launch on the host instead of a
+        // dozen.
+        if (graphSingle == nullptr || graphSingleVersion != configVersion)
+        {
+            if (graphSingle)
+            {
+                cudaGraphExecDestroy(graphSingle);
+                graphSingle = nullptr;
+            }
+            const uint64_t before = launchCount();
+            CRB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            r = invalidateRecords();
+            if (r == CRB200_OK)
+                r = launchStep();
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            const uint64_t captured = launchCount() - before;
+            noteLaunches((uint64_t)0 - captured); // captured, not yet executed
+            if (r != CRB200_OK)
+            {
+                if (g)
+                    cudaGraphDestroy(g);
+                return r;
+            }
+            if (e != cudaSuccess)
+                return cudaFail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&graphSingle, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess)
+                return cudaFail(e, "cudaGraphInstantiate");
+            graphSingleKernels = (int)captured;
+            graphSingleVersion = configVersion;
+        }
+        CRB_CHECK(cudaGraphLaunch(graphSingle, stream));
+        noteLaunches((uint64_t)graphSingleKernels);
+        return CRB200_OK;
     }
 
     // Bins and P2G records written by G2P hold for the next substep of the same call only: the
@@ -2433,7 +2476,8 @@ namespace crb200
             CRB_CHECK(cudaMalloc(&onesMask, n));
             CRB_CHECK(cudaMalloc(&iotaIds, n * sizeof(unsigned)));
             CRB_CHECK(cudaMemsetAsync(onesMask, 1, n, stream));
-            k_iota<<<strideCtas, 256, 0, stream>>>((unsigned)n, iotaIds);
+            // (may run before initialize(), so the grid is sized here)
+            k_iota<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, stream>>>((unsigned)n, iotaIds);
             CRB_LAUNCHED(1);
         }
         if (stdGpuSemantics != on)

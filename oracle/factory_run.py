@@ -109,11 +109,11 @@ def build(lib, scene, spare):
     obj = lib.CrCreateParticleObject(spacing, rho * spacing ** 3, geo, C.byref(pos), C.byref(rot), C.byref(one),
                                      MAT_NEOHOOKEAN, C.byref(mp), C.byref(n))
     nmax = int(n.value * max(spare, 1.0))
-    # The slab's gravity leans a little (0.3 degrees) so that no grid node next to a pin moves
-    # exactly parallel to the pin's face: the reference applies contact only to nodes that approach
-    # a shape (mpm_rigid_contact.h:187-191), and on the particle lattice of a slab at rest the
-    # horizontal node velocities would otherwise be rounding noise whose sign decides it.
-    g = Vec3(0, -9.81, 0) if scene.startswith("cube") else Vec3(0.05, -9.81, 0.03)
+    # Gravity leans a little (0.3 degrees) so that no grid node next to a shape moves exactly
+    # parallel to its face: the reference applies contact only to nodes that approach a shape
+    # (mpm_rigid_contact.h:187-191), and on a particle lattice at rest the tangential node
+    # velocities would otherwise be rounding noise whose sign decides it (and friction with them).
+    g = Vec3(0.05, -9.81, 0.03)
     sc = lib.CrCreateScene(SOLVER[scene], nmax, g, bounds, cell, dt, iterations, 0)
     off = C.c_uint(0)
     lib.CrAddParticleObjectToScene(obj, sc, C.byref(off))
@@ -157,6 +157,12 @@ def main():
         raise SystemExit("CrInitializeEngine failed")
     sc, shapes, n, nmax, dt = build(lib, scene, spare)
     frame_dt = substeps * dt
+    # the substeps SceneImpl runs per frame: `while (t < dt) t += step()` in float
+    # (scene_impl.cpp:313-317), which can run one more than frame_dt / dt
+    t, per_frame = np.float32(0.0), 0
+    while t < np.float32(frame_dt):
+        t = np.float32(t + np.float32(dt))
+        per_frame += 1
 
     def particles(pd, count):
         x = np.ctypeslib.as_array(C.cast(pd.positionMass, C.POINTER(C.c_float)), shape=(count, 4)).copy()
@@ -180,10 +186,11 @@ def main():
         lib.CrGetShapeCouplingForceTorque(s, C.byref(f), C.byref(tq))
         ft.append([f.x, f.y, f.z, tq.x, tq.y, tq.z])
     np.savez(out, x0=x0, x=x, v=v, times=np.array(times), n=n, nmax=nmax, coupling=np.array(ft, np.float64),
-             substeps=substeps)
+             substeps=per_frame)
     lib.CrReleaseScene(sc)
     lib.CrReleaseEngine()
-    print(f"{scene} n={n} nmax={nmax} frames={frames} median frame {np.median(times) * 1e3:.3f} ms")
+    print(f"{scene} n={n} nmax={nmax} frames={frames} substeps per frame {per_frame} "
+          f"median frame {np.median(times) * 1e3:.3f} ms")
 
 
 if __name__ == "__main__":

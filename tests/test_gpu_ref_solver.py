@@ -147,7 +147,8 @@ def test_standard_mpm_inactive_particles_as_the_reference_gpu_solver(tmp_path):
         g.step(steps)
         out[on] = g.state()
     x0 = sc.pos_mass[:, :3]
-    assert float(np.abs(ref["x"][k:] - x0[k:]).max()) > 1e-3, "the reference left the switched-off particles"
+    # 10 ms of fall: about 0.5 mm
+    assert float(np.abs(ref["x"][k:] - x0[k:]).max()) > 2e-4, "the reference left the switched-off particles"
     e = rel_pos_err(out[True]["x"], ref["x"], x0, sc.cell_size)
     assert e <= 1e-4, f"engine with the GPU solver's semantics vs reference CUDA: {e:.3e}"
     np.testing.assert_array_equal(out[False]["x"][k:], x0[k:])
