@@ -585,7 +585,9 @@ def adjoint_scene(kind: str = "plane", seed: int = 1006, side: float = 0.1, cell
 
     kind "plane": the ground plane only.  kind "mixed": the plane, a kinematic sphere (translating
     and spinning), a static box and a tilted static capsule around the impact point, with smoothing
-    distances and drags that put grid nodes in every contact branch.
+    distances and drags that put grid nodes in every contact branch.  kind "effmass": the
+    effective-mass contact model, the plane and a rotated, moving dynamic sphere with mass and
+    inertia next to the impact point (two-body impulses with friction, both friction branches).
     """
     sc = material_cube(seed=seed, side=side, cell=cell, E=E, nu=nu, v0=v0, drop=0.005)
     if kind == "mixed":
@@ -601,6 +603,17 @@ def adjoint_scene(kind: str = "plane", seed: int = 1006, side: float = 0.1, cell
         c, s_ = math.cos(0.6), math.sin(0.6)
         st.add_shape(g, SHAPE_STATIC, (0.0, 0.0, -0.04), rotation=(s_, 0, 0, c), smooth=0.02, drag=0.9, friction=0.2)
         sc.shapes = st
+    elif kind == "effmass":
+        st = ShapeTable.empty()
+        g = st.add_geometry(GEOM_PLANE, (0, 0, 0, 0))
+        st.add_shape(g, SHAPE_STATIC, (0, 0, 0), friction=0.3)
+        g = st.add_geometry(GEOM_SPHERE, (0.04, 0, 0, 0))
+        c, s_ = math.cos(0.4), math.sin(0.4)
+        st.add_shape(g, SHAPE_DYNAMIC, (0.035, -0.015, 0.01), rotation=(0, s_, 0, c), smooth=0.02, drag=0.7,
+                     friction=0.4, lin_vel=(0, 0.1, 0), ang_vel=(0.5, 0, 1.0), com_inv_mass=(0.01, 0.0, -0.005, 4.0),
+                     inertia0=(300.0, 250.0, 200.0, 0), inertia1=(10.0, 5.0, 2.0, 0))
+        sc.shapes = st
+        sc.contact_model = 1
     elif kind != "plane":
         raise ValueError(kind)
     sc.name = f"adjoint_{kind}"

@@ -397,6 +397,113 @@ namespace crb200
     }
 
     // ---------------------------------------------------------------------------------------
+    // The effective-mass response of a dynamic shape to one grid node (mpm_rigid_contact.h:219-320,
+    // as rigidContact computes it) and what its reverse needs.  ok = false: the impulse is
+    // undefined (non-positive inverse masses) and the node velocity becomes zero (:231).
+    struct EffMassHit
+    {
+        bool ok, hasT, caseA;
+        V3 rr, w, vt, e, tot;
+        float imc, Jn, vtn, fJt, fin, totJt;
+    };
+    __device__ __forceinline__ V3 effMassResponse(const ShapeRec &r, V3 v, float m, V3 wrel, V3 nrm, V3 rel, float vn,
+                                                  EffMassHit &h)
+    {
+        h.ok = false;
+        const float imR = r.comInvMass.w;
+        if (!(imR > 0.f))
+            return v3(0.f, 0.f, 0.f);
+        h.rr = wrel - qrot(r.rot, v3(r.comInvMass));
+        const V3 rxnl = qrotInv(r.rot, cross(h.rr, nrm));
+        const V3 wl = v3(r.inertia0.x * rxnl.x + r.inertia1.x * rxnl.y + r.inertia1.y * rxnl.z,
+                         r.inertia1.x * rxnl.x + r.inertia0.y * rxnl.y + r.inertia1.z * rxnl.z,
+                         r.inertia1.y * rxnl.x + r.inertia1.z * rxnl.y + r.inertia0.z * rxnl.z);
+        h.w = qrot(r.rot, wl); // world inverse inertia times (r x n)
+        const V3 tt = cross(h.w, h.rr);
+        const float invMassGrid = 1.f / m;
+        h.imc = invMassGrid + (imR + dot(nrm, tt));
+        if (!(h.imc > 0.f))
+            return v3(0.f, 0.f, 0.f);
+        h.ok = true;
+        h.Jn = -1.f * vn / h.imc;
+        h.vt = rel - nrm * vn;
+        h.vtn = sqrtf(sq(h.vt));
+        h.hasT = h.vtn > kEps;
+        V3 impT = v3(0.f, 0.f, 0.f);
+        h.totJt = 0.f;
+        h.e = v3(0.f, 0.f, 0.f);
+        h.fJt = 0.f;
+        h.fin = 0.f;
+        h.caseA = false;
+        if (h.hasT)
+        {
+            const float capA = r.params0.z * h.Jn, capB = h.vtn / h.imc;
+            h.caseA = capA <= capB;
+            h.fJt = fminf(capA, capB);
+            h.fin = (h.vtn - h.fJt * h.imc) * r.params0.y;
+            h.totJt = (h.vtn - h.fin) / h.imc;
+            h.e = h.vt * (1.f / h.vtn);
+            impT = (h.vt * -1.f / h.vtn) * h.totJt;
+        }
+        h.tot = nrm * h.Jn + impT;
+        return v + h.tot * invMassGrid;
+    }
+
+    // Reverse of effMassResponse for g = dL/dresp: returns dL/dv (input velocity) and adds
+    // dL/dn, dL/drel's rigid part (through gvr), dL/dr and dL/dm.
+    __device__ __forceinline__ V3 effMassReverse(const ShapeRec &r, const EffMassHit &h, V3 g, float m, V3 nrm, V3 rel,
+                                                 float vn, V3 &gn, V3 &grr, V3 &gvr, float &gm)
+    {
+        gn = v3(0.f, 0.f, 0.f);
+        grr = v3(0.f, 0.f, 0.f);
+        gvr = v3(0.f, 0.f, 0.f);
+        if (!h.ok)
+            return v3(0.f, 0.f, 0.f); // resp = 0 whatever the input
+        const float im = 1.f / m, imc = h.imc, s = r.params0.y, mu = r.params0.z;
+        V3 gvin = g;                                       // resp = v + tot / m
+        const V3 gtot = g * im;
+        gm += -dot(g, h.tot) * im * im;
+        float gJn = dot(gtot, nrm);                        // tot = n Jn + impT
+        gn = gtot * h.Jn;
+        V3 ge = v3(0.f, 0.f, 0.f);
+        float gtotJt = 0.f;
+        if (h.hasT)
+        {
+            ge = gtot * (-h.totJt);                        // impT = -e totJt
+            gtotJt = -dot(gtot, h.e);
+        }
+        float gvtn = gtotJt / imc;                         // totJt = (vtn - fin) / imc
+        const float gfin = -gtotJt / imc;
+        float gimc = -gtotJt * (h.vtn - h.fin) / (imc * imc);
+        gvtn += gfin * s;                                  // fin = (vtn - fJt imc) s
+        const float gfJt = -gfin * s * imc;
+        gimc += -gfin * s * h.fJt;
+        if (h.caseA)                                       // fJt = min(mu Jn, vtn / imc)
+            gJn += gfJt * mu;
+        else
+        {
+            gvtn += gfJt / imc;
+            gimc += -gfJt * h.vtn / (imc * imc);
+        }
+        V3 gvt = v3(0.f, 0.f, 0.f);
+        if (h.hasT)
+            gvt = (ge - h.e * dot(h.e, ge)) * (1.f / h.vtn) + h.e * gvtn; // e = vt / vtn, vtn = |vt|
+        float gvn = -gJn / imc;                            // Jn = -vn / imc
+        gimc += gJn * vn / (imc * imc);
+        V3 grel = gvt;                                     // vt = rel - n vn
+        gn = gn - gvt * vn;
+        gvn -= dot(gvt, nrm);
+        grel = grel + nrm * gvn;                           // vn = rel . n
+        gn = gn + rel * gvn;
+        gm += -gimc * im * im;                             // imc = 1 / m + imr
+        const V3 gu = h.w * (2.f * gimc);                  // imr = m_R^-1 + u^T Iw u, Iw u = w
+        grr = cross(nrm, gu);                              // u = rr x n
+        gn = gn + cross(gu, h.rr);
+        gvin = gvin + grel;                                // rel = v - vr
+        gvr = grel * -1.f;
+        return gvin;
+    }
+
     // Reverse of the grid update (per touched node): gridG (dL/dV_n) -> (dL/dP_n, dL/dM_n).
     // Clears gridA for the next replayed P2G.
     template <bool Multi>
@@ -441,6 +548,7 @@ namespace crb200
             const V3 pos = v3((float)i * g.dx, (float)j * g.dx, (float)k * g.dx) + v3(g.gmin.x, g.gmin.y, g.gmin.z) +
                            v0 * p.dt;
             // forward contact chain: velocity before each active contact
+            const bool effMass = p.contactModel == CRB200_CONTACT_EFFECTIVE_MASS;
             V3 vin[kAdjMaxHits];
             int hs[kAdjMaxHits];
             int nh = 0;
@@ -460,15 +568,21 @@ namespace crb200
                 const float vn = dot(rel, nrm);
                 if (vn >= 0.f)
                     continue;
-                const V3 tang = rel - nrm * vn;
-                const float tn = sqrtf(sq(tang));
-                const float fc = fmaxf(r.params0.z * vn / (tn + kEps), -1.f);
                 if (nh < kAdjMaxHits)
                 {
                     vin[nh] = v;
                     hs[nh] = s;
                     ++nh;
                 }
+                if (effMass && r.kind == S_DYNAMIC)
+                {
+                    EffMassHit h;
+                    v = effMassResponse(r, v, acc.w, wrel, nrm, rel, vn, h);
+                    continue;
+                }
+                const V3 tang = rel - nrm * vn;
+                const float tn = sqrtf(sq(tang));
+                const float fc = fmaxf(r.params0.z * vn / (tn + kEps), -1.f);
                 v = (tang + tang * fc) * r.params0.y + rv;
             }
             // boundary band
@@ -479,6 +593,7 @@ namespace crb200
             if (k < 2 || k > g.n.z - 3)
                 gv.z = 0.f;
             V3 gpos = v3(0.f, 0.f, 0.f);
+            float gmEff = 0.f; // dL/dm through the effective-mass responses
             for (int h = nh - 1; h >= 0; --h)
             {
                 const ShapeRec &r = shp[hs[h]];
@@ -489,6 +604,19 @@ namespace crb200
                 const V3 rv = r.kind == S_STATIC ? v3(0.f, 0.f, 0.f) : v3(r.linVel) + cross(v3(r.angVel), wrel);
                 const V3 rel = vin[h] - rv;
                 const float vn = dot(rel, nrm);
+                if (effMass && r.kind == S_DYNAMIC)
+                {
+                    EffMassHit eh;
+                    (void)effMassResponse(r, vin[h], acc.w, wrel, nrm, rel, vn, eh);
+                    V3 gn, grr, gvr;
+                    gv = effMassReverse(r, eh, gv, acc.w, nrm, rel, vn, gn, grr, gvr, gmEff);
+                    if (eh.ok)
+                    {
+                        adjNormalJacobian(r, lp, gl, J);
+                        gpos = gpos + adjJtG(J, gn) + grr + cross(gvr, v3(r.angVel));
+                    }
+                    continue;
+                }
                 const V3 tang = rel - nrm * vn;
                 const float tn = sqrtf(sq(tang));
                 const float fr = r.params0.z, sticky = r.params0.y;
@@ -519,7 +647,7 @@ namespace crb200
             }
             const V3 gv0 = gv + gpos * p.dt;
             const float im = 1.f / acc.w;
-            gridG[a] = make_float4(gv0.x * im, gv0.y * im, gv0.z * im, -dot(gv0, v0) * im);
+            gridG[a] = make_float4(gv0.x * im, gv0.y * im, gv0.z * im, -dot(gv0, v0) * im + gmEff);
         }
     }
 
@@ -801,8 +929,8 @@ namespace crb200
         return CRB200_OK;
     }
 
-    // What the adjoint differentiates: MLS-MPM, kinematic contact model, Neo-Hookean active
-    // particles, analytic shapes of uniform scale.  Reads the (small) shape table and the particle
+    // What the adjoint differentiates: MLS-MPM, the kinematic and effective-mass contact models,
+    // Neo-Hookean active particles, analytic shapes of uniform scale.  Reads the (small) shape table and the particle
     // material types / mask back to the host once per recording.
     int Solver::adjointCheck()
     {
@@ -812,9 +940,9 @@ namespace crb200
             return CRB200_ERR_UNSUPPORTED;
         }
         for (const StepParams &sp : allParams())
-            if (sp.contactModel != CRB200_CONTACT_KINEMATIC)
+            if (sp.contactModel != CRB200_CONTACT_KINEMATIC && sp.contactModel != CRB200_CONTACT_EFFECTIVE_MASS)
             {
-                setLastError("adjoint: only the kinematic contact model is differentiated");
+                setLastError("adjoint: unknown contact model");
                 return CRB200_ERR_UNSUPPORTED;
             }
         const unsigned n = totalParticles();

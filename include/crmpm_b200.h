@@ -393,9 +393,10 @@ CRB200_API int CrB200BatchCreate(int solverType, int numScenes, const CrB200Batc
  * captureSubsteps (host, numCaptures entries, strictly increasing in [1, numSubsteps]) lists the
  * substeps whose positions are copied, as float4 (x, y, z, m), into capturedPositions (device,
  * numCaptures x numParticles entries, capture-major).  The solver is left in the final state.
- * Differentiated: the MLS-MPM solver, Neo-Hookean active particles, the kinematic contact model,
- * box / sphere / plane / capsule shapes of uniform scale (anything else is refused with
- * CRB200_ERR_UNSUPPORTED).  Works on single-scene solvers and batches alike. */
+ * Differentiated: the MLS-MPM solver, Neo-Hookean active particles, the kinematic and the
+ * effective-mass contact models, box / sphere / plane / capsule shapes of uniform scale (anything
+ * else, slicers included, is refused with CRB200_ERR_UNSUPPORTED).  Works on single-scene solvers
+ * and batches alike. */
 CRB200_API int CrB200SolverAdjointRecord(CrB200SolverHandle solver, int numSubsteps, int checkpointInterval,
                                          int numCaptures, const int *captureSubsteps,
                                          CrB200Float4 *capturedPositions);

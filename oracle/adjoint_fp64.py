@@ -16,9 +16,10 @@ Forward arithmetic followed (reference file:line):
   * G2P: v, C = 4/dx sum w d v^T (the reference's transposed outer product), x += v dt clamped to
     the grid bounds, F <- (I + dt C) F        mls_mpm_algorithm.h:296-390
 
-Scope (the same as the GPU adjoint): MLS-MPM, Neo-Hookean particles, kinematic contact model,
-static / kinematic / dynamic shapes of analytic geometry (box, sphere, plane, capsule) with uniform
-scale, no slicers.  Branch decisions (contact on/off, friction clamp, position clamp, grid mass
+Scope (the same as the GPU adjoint): MLS-MPM, Neo-Hookean particles, the kinematic and the
+effective-mass contact models (mpm_rigid_contact.h:219-320: two-body normal and friction impulses
+against dynamic shapes), static / kinematic / dynamic shapes of analytic geometry (box, sphere,
+plane, capsule) with uniform scale, no slicers.  Branch decisions (contact on/off, friction clamp, position clamp, grid mass
 cutoff) are held fixed when differentiating.
 
 State layout: x, v (N, 3); F, C (N, 3, 3) with F[p, r, c] = F(r, c).
@@ -62,6 +63,14 @@ class _Shape:
         self.ang = st.ang_vel[sid, :3].astype(np.float64)
         smooth, drag, friction, fatten = (float(t) for t in st.params0[sid])
         self.smooth, self.drag, self.friction, self.fatten = smooth, drag, friction, fatten
+        # dynamic shapes under the effective-mass model: centre of mass (local), inverse mass and
+        # the world inverse inertia R I^-1 R^T (inertiaInv0 = diagonal, inertiaInv1 = xy, xz, yz;
+        # mpm_rigid_contact.h:84-94)
+        self.com = st.com_inv_mass[sid, :3].astype(np.float64)
+        self.inv_mass = float(st.com_inv_mass[sid, 3])
+        d0, d1 = st.inertia0[sid].astype(np.float64), st.inertia1[sid].astype(np.float64)
+        Iloc = np.array([[d0[0], d1[0], d1[1]], [d1[0], d0[1], d1[2]], [d1[1], d1[2], d0[2]]])
+        self.Iw = self.R @ Iloc @ self.R.T
 
     def eval(self, pos):
         """dist (K,), unit normal n (K,3) and dn/dpos (K,3,3) at world points (mpm_rigid_contact.h:129-148)."""
@@ -133,8 +142,9 @@ class Fp64Adjoint:
 
         if scene.solver_type != S.SOLVER_MLS:
             raise NotImplementedError("adjoint: MLS-MPM only")
-        if scene.contact_model != 0:
-            raise NotImplementedError("adjoint: kinematic contact model only")
+        if scene.contact_model not in (0, 1):
+            raise NotImplementedError("adjoint: kinematic or effective-mass contact model only")
+        self.eff_mass = scene.contact_model == 1
         if not np.all(scene.mat_type == S.MAT_NEOHOOKEAN):
             raise NotImplementedError("adjoint: Neo-Hookean particles only")
         self.sc = scene
@@ -220,6 +230,7 @@ class Fp64Adjoint:
         pos = self.node_ijk[idx] * self.dx + self.gmin[None] + v0 * self.dt
         v = v0.copy()
         steps = []
+        Mh = M[idx]
         for sh in self.shapes:
             dist, n, Jn = sh.eval(pos)
             vr = sh.rigid_vel(pos)
@@ -228,12 +239,18 @@ class Fp64Adjoint:
             act = (dist < sh.smooth) & (vn < 0.0)
             t = rel - n * vn[:, None]
             tn = np.sqrt((t * t).sum(1))
-            arg = sh.friction * vn / (tn + EPS)
-            fc = np.maximum(arg, -1.0)
-            resp = (t + t * fc[:, None]) * sh.drag + vr
-            if tape:
-                steps.append(dict(sh=sh, n=n, Jn=Jn, rel=rel, vn=vn, act=act, t=t, tn=tn, fc=fc,
-                                  clamped=arg <= -1.0))
+            if self.eff_mass and sh.kind == 2:
+                em = self._eff_mass_forward(sh, pos, n, v, rel, vn, t, tn, Mh)
+                resp = em["resp"]
+                if tape:
+                    steps.append(dict(sh=sh, n=n, Jn=Jn, rel=rel, vn=vn, act=act, t=t, tn=tn, em=em, v=v))
+            else:
+                arg = sh.friction * vn / (tn + EPS)
+                fc = np.maximum(arg, -1.0)
+                resp = (t + t * fc[:, None]) * sh.drag + vr
+                if tape:
+                    steps.append(dict(sh=sh, n=n, Jn=Jn, rel=rel, vn=vn, act=act, t=t, tn=tn, fc=fc,
+                                      clamped=arg <= -1.0))
             v = np.where(act[:, None], resp, v)
         ijk = self.node_ijk[idx]
         bc = np.stack([(ijk[:, k] < 2) | (ijk[:, k] > self.n[k] - 3) for k in range(3)], 1)
@@ -242,6 +259,93 @@ class Fp64Adjoint:
         if tape:
             return V, dict(idx=idx, v0=v0, M=M[idx], P=P[idx], steps=steps, bc=bc)
         return V
+
+    def _eff_mass_forward(self, sh, pos, n, v, rel, vn, vt, vtn, M):
+        """Effective-mass response of a dynamic shape (mpm_rigid_contact.h:219-320): the normal and
+        friction impulses of a two-body contact between the node (mass M) and the rigid body; the
+        node velocity is zero where the impulse is undefined (non-positive inverse masses, :231)."""
+        K = pos.shape[0]
+        out = dict(ok=np.zeros(K, bool), resp=np.zeros((K, 3)))
+        if sh.inv_mass <= 0.0:
+            return out
+        rr = (pos - sh.p[None]) - (sh.R @ sh.com)[None]
+        u = np.cross(rr, n)
+        imr = sh.inv_mass + np.einsum("ki,ij,kj->k", u, sh.Iw, u)
+        imc = 1.0 / M + imr
+        ok = imc > 0.0
+        imc_s = np.where(ok, imc, 1.0)
+        Jn = -vn / imc_s
+        has_t = vtn > EPS
+        vtn_s = np.where(has_t, vtn, 1.0)
+        capA = sh.friction * Jn
+        capB = vtn / imc_s
+        caseA = capA <= capB
+        fJt = np.where(caseA, capA, capB)
+        fin = (vtn - fJt * imc_s) * sh.drag
+        totJt = (vtn - fin) / imc_s
+        e = vt / vtn_s[:, None]
+        impT = np.where(has_t[:, None], -e * totJt[:, None], 0.0)
+        tot = n * Jn[:, None] + impT
+        resp = v + tot / M[:, None]
+        out.update(ok=ok, resp=np.where(ok[:, None], resp, 0.0), rr=rr, u=u, imr=imr, imc=imc_s, Jn=Jn,
+                   has_t=has_t, vtn=vtn_s, caseA=caseA, fJt=fJt, fin=fin, totJt=totJt, e=e, tot=tot, M=M)
+        return out
+
+    def _eff_mass_reverse(self, sh, st, g):
+        """Reverse of _eff_mass_forward for gradient g = dL/dresp: (dL/dv_in, dL/dpos, dL/dM)."""
+        em = st["em"]
+        K = g.shape[0]
+        gv_in = np.zeros((K, 3))
+        gpos = np.zeros((K, 3))
+        gM = np.zeros(K)
+        if sh.inv_mass <= 0.0:
+            return gv_in, gpos, gM
+        ok = em["ok"][:, None]
+        g = np.where(ok, g, 0.0)
+        n, rel, vn, vt, M = st["n"], st["rel"], st["vn"], st["t"], em["M"]
+        imc, Jn, vtn, e, totJt, fJt, fin = em["imc"], em["Jn"], em["vtn"], em["e"], em["totJt"], em["fJt"], em["fin"]
+        has_t = em["has_t"]
+        s_, mu = sh.drag, sh.friction
+        gv_in += g                                   # resp = v + tot / M
+        gtot = g / M[:, None]
+        gM += -(g * em["tot"]).sum(1) / M ** 2
+        gJn = (gtot * n).sum(1)                      # tot = n Jn + impT
+        gn = gtot * Jn[:, None]
+        ge = np.where(has_t[:, None], -gtot * totJt[:, None], 0.0)   # impT = -e totJt
+        gtotJt = np.where(has_t, -(gtot * e).sum(1), 0.0)
+        gvtn = gtotJt / imc                          # totJt = (vtn - fin) / imc
+        gfin = -gtotJt / imc
+        gimc = -gtotJt * (vtn - fin) / imc ** 2
+        gvtn += gfin * s_                            # fin = (vtn - fJt imc) s
+        gfJt = -gfin * s_ * imc
+        gimc += -gfin * s_ * fJt
+        caseA = em["caseA"]                          # fJt = min(mu Jn, vtn / imc)
+        gJn += np.where(caseA, gfJt * mu, 0.0)
+        gvtn += np.where(caseA, 0.0, gfJt / imc)
+        gimc += np.where(caseA, 0.0, -gfJt * vtn / imc ** 2)
+        gvt = (ge - e * (e * ge).sum(1, keepdims=True)) / vtn[:, None]   # e = vt / vtn
+        gvt += gvtn[:, None] * e                     # vtn = |vt|
+        gvt = np.where(has_t[:, None], gvt, 0.0)
+        gvn = -gJn / imc                             # Jn = -vn / imc
+        gimc += gJn * vn / imc ** 2
+        grel = gvt.copy()                            # vt = rel - n vn
+        gn += -gvt * vn[:, None]
+        gvn += -(gvt * n).sum(1)
+        grel += gvn[:, None] * n                     # vn = rel . n
+        gn += gvn[:, None] * rel
+        gM += -gimc / M ** 2                         # imc = 1 / M + imr
+        gimr = gimc
+        gu = 2.0 * (em["u"] @ sh.Iw.T) * gimr[:, None]   # imr = m^-1 + u^T Iw u (Iw symmetric)
+        rr = em["rr"]
+        grr = np.cross(n, gu)                        # u = rr x n
+        gn += np.cross(gu, rr)
+        gpos += grr                                  # rr = pos - p - R com
+        gv_in += grel                                # rel = v - vr
+        gvr = -grel
+        gpos += np.einsum("kji,kj->ki", st["Jn"], gn)
+        if sh.kind != 0:
+            gpos += np.cross(gvr, sh.ang[None])
+        return gv_in, gpos, gM
 
     def _push_out(self, xs, tape: bool = False):
         steps = []
@@ -345,9 +449,16 @@ class Fp64Adjoint:
         idx = gt["idx"]
         gv_ = np.where(gt["bc"], 0.0, gV[idx])
         gpos = np.zeros_like(gv_)
+        gM_eff = np.zeros(gv_.shape[0])
         for st in reversed(gt["steps"]):
             sh = st["sh"]
             act = st["act"]
+            if "em" in st:
+                gvi, gpi, gmi = self._eff_mass_reverse(sh, st, gv_)
+                gv_ = np.where(act[:, None], gvi, gv_)
+                gpos = gpos + np.where(act[:, None], gpi, 0.0)
+                gM_eff += np.where(act, gmi, 0.0)
+                continue
             n, rel, vn_, tt, tn, fc = st["n"], st["rel"], st["vn"], st["t"], st["tn"], st["fc"]
             gr = gv_
             free = ~st["clamped"]
@@ -372,7 +483,7 @@ class Fp64Adjoint:
         gv0 = gv_ + dt * gpos
         Mi = gt["M"]
         gP[idx] = gv0 / Mi[:, None]
-        gM[idx] = -(gv0 * gt["v0"]).sum(1) / Mi
+        gM[idx] = -(gv0 * gt["v0"]).sum(1) / Mi + gM_eff
         # ---- P2G reverse
         gPn = gP[flat] * valid[..., None]
         gMn = gM[flat] * valid

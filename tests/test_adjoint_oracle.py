@@ -17,7 +17,7 @@ STEPS = 30
 CAPS = (10, 20, 30)
 
 
-@pytest.mark.parametrize("kind", ["plane", "mixed"])
+@pytest.mark.parametrize("kind", ["plane", "mixed", "effmass"])
 def test_fp64_forward_matches_oracle(kind):
     sc = scenes.adjoint_scene(kind)
     a = Fp64Adjoint(sc)
@@ -38,7 +38,7 @@ def test_fp64_forward_matches_oracle(kind):
     np.testing.assert_allclose(a.V0, st["V0"], rtol=1e-12)
 
 
-@pytest.mark.parametrize("kind", ["plane", "mixed"])
+@pytest.mark.parametrize("kind", ["plane", "mixed", "effmass"])
 def test_fp64_adjoint_matches_central_differences(kind):
     sc = scenes.adjoint_scene(kind)
     n = sc.n

@@ -4,7 +4,8 @@ torch.autograd.Function wrapper.
 The reference has no gradient path.  The GPU gradients (float32) are compared with the FP64 host
 adjoint (oracle/adjoint_fp64.py), which the CPU tests pin to central finite differences within
 1e-5: dL/dE, dL/dnu and the summed dL/dv0 within 1e-3 relative, per-particle dL/dv0 within 1e-2
-relative L2.  Central finite differences of the GPU forward itself, all in deterministic mode
+relative L2, with the kinematic contact model and with the effective-mass model (two-body impulses
+against a dynamic shape).  Central finite differences of the GPU forward itself, all in deterministic mode
 (CRB200_OPT_DETERMINISTIC, which the backward pass's replays follow), are checked within 1e-3 for
 E, nu and v0 on the small cube, and for E and nu over the 200 substeps of the
 material-identification workload (64k particles), whose gradients are also checked against the
@@ -67,7 +68,7 @@ def _run(sc):
     return ds, Trajectory(ds, STEPS, CAPS, checkpoint_interval=8)
 
 
-@pytest.mark.parametrize("kind", ["plane", "mixed"])
+@pytest.mark.parametrize("kind", ["plane", "mixed", "effmass"])
 def test_gpu_adjoint_matches_fp64_adjoint(kind):
     sc = scenes.adjoint_scene(kind)
     a, xs, tgt = _targets(sc)
