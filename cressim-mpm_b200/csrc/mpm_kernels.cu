@@ -684,7 +684,10 @@ namespace crb200
         // touchedFlag (resident path): the block's "already listed" flag, cleared as it is consumed
         __shared__ ShapeRec sh[Multi ? 1 : kMaxShapes];
         __shared__ unsigned sTouched;
-        __shared__ float sCouple[Det ? 256 : 1][kDetSlots * 6]; // Det: one row of coupling sums per thread
+        // Det (single scene): one row of coupling sums per thread.  A batch keeps the coupling
+        // atomics: its tiles make the particle state reproducible, not the shapes' force sums.
+        constexpr bool kRows = Det > 0 && !Multi;
+        __shared__ float sCouple[kRows ? 256 : 1][kDetSlots * 6];
         if (threadIdx.x == 0)
             sTouched = 0;
         if (!Multi && p0.numShapes > 0)
@@ -693,15 +696,15 @@ namespace crb200
         const unsigned nT = hdr->numTouchedBlocks;
         const bool withForce = p0.solverType == CRB200_SOLVER_GPU_STANDARD;
         const unsigned perCta = blockDim.x / 64;
-        using Couple = typename std::conditional<(Det > 0), CoupleRow, CoupleAtomic>::type;
-        if constexpr (Det > 0)
+        using Couple = typename std::conditional<kRows, CoupleRow, CoupleAtomic>::type;
+        if constexpr (kRows)
             for (int c = 0; c < kDetSlots * 6; ++c)
                 sCouple[threadIdx.x][c] = 0.f;
         for (unsigned base = blockIdx.x * perCta; base < nT; base += gridDim.x * perCta)
         {
             const unsigned bi = base + threadIdx.x / 64;
             Couple couple;
-            if constexpr (Det > 0)
+            if constexpr (kRows)
                 couple = CoupleRow{sCouple[threadIdx.x], CoupleAtomic{coupleForce, coupleTorque}, false};
             else
                 couple = CoupleAtomic{coupleForce, coupleTorque};
@@ -789,7 +792,7 @@ namespace crb200
                 if (saveV)
                     saveV[a] = make_float4(v.x, v.y, v.z, acc.w);
             } while (false);
-            if constexpr (Det > 0)
+            if constexpr (kRows)
             {
                 // block sums in a fixed order: thread c < 24 of each 64-thread group adds column c
                 // of the group's rows in row order, writes it and clears the column
@@ -1361,14 +1364,17 @@ namespace crb200
             atomicMax(maxBits, __float_as_uint(m)); // positive floats order like their bits
     }
 
-    __global__ void k_initMassFixed(GridGeom g, unsigned n, const unsigned *__restrict__ idx, const float4 *__restrict__ xm,
-                                    float *__restrict__ F, unsigned stride, const unsigned *__restrict__ maxBits,
-                                    unsigned long long *__restrict__ fixedMass)
+    __global__ void k_initMassFixed(GridGeom g0, SceneTable sc, unsigned n, const unsigned *__restrict__ idx,
+                                    const float4 *__restrict__ xm, float *__restrict__ F, unsigned stride,
+                                    const unsigned *__restrict__ maxBits, unsigned long long *__restrict__ fixedMass)
     {
         const unsigned ii = blockIdx.x * blockDim.x + threadIdx.x;
         if (ii >= n)
             return;
         const unsigned p = idx[ii];
+        if (sc.particleScene && sc.particleScene[p] == 0xFFFFu)
+            return;
+        const GridGeom g = sc.particleScene ? sc.params[sc.particleScene[p]].g : g0;
         M3 I;
 #pragma unroll
         for (int e = 0; e < 9; ++e)
@@ -1824,7 +1830,9 @@ namespace crb200
     int Solver::detLevel(bool recomputing) const
     {
         (void)recomputing;
-        if (isBatch() || !detPartials)
+        if (isBatch())
+            return (detP2G && detTiles) ? 2 : 0; // a batch has no fixed-order coupling
+        if (!detPartials)
             return 0;
         if (detP2G && detTiles)
             return 2;
@@ -1835,13 +1843,9 @@ namespace crb200
     // solver's force pass), written whole by the accumulation of each active block.
     int Solver::setDeterministic(bool on)
     {
-        if (on && isBatch())
-        {
-            setLastError("deterministic substeps: not available on batch solvers");
-            return CRB200_ERR_UNSUPPORTED;
-        }
-        if (int rc = setDeterministicCoupling(on))
-            return rc;
+        if (!isBatch())
+            if (int rc = setDeterministicCoupling(on))
+                return rc;
         if (on && !detTiles)
         {
             const size_t bytes = (size_t)totalBlocks * kTileNodes * sizeof(float4);
@@ -2079,7 +2083,7 @@ namespace crb200
         int r = sortParticles(p, isStd);
         if (r != CRB200_OK)
             return r;
-        if (!Multi && nPart > 0 && detLevel(recompute || adjReplay) == 2)
+        if (nPart > 0 && detLevel(recompute || adjReplay) == 2)
         {
             k_cellOrder<<<cellCtas * 4, 64, 0, stream>>>(header, activeList, blockStart, cellStart, sortedIds);
             CRB_LAUNCHED(1);
@@ -2095,14 +2099,13 @@ namespace crb200
                                                         F, Cm, V0, stride, cutMasks, records, gridA, gridF,
                                                         &header->fp64Fallbacks);
             bool tiled = false;
-            if constexpr (!Multi)
-                if (detLevel(recompute || adjReplay) == 2)
-                {
-                    k_accumulate<M, false, true><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart,
-                                                                           sortedIds, cellStart, records, cutMasks,
-                                                                           gridA, gridF, detTiles, detTilesF);
-                    tiled = true;
-                }
+            if (detLevel(recompute || adjReplay) == 2)
+            {
+                k_accumulate<M, Multi, true><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart,
+                                                                       sortedIds, cellStart, records, cutMasks,
+                                                                       gridA, gridF, detTiles, detTilesF);
+                tiled = true;
+            }
             if (!tiled)
                 k_accumulate<M, Multi><<<p2gCtas, 64, 0, stream>>>(p, sc, header, activeList, blockStart, sortedIds,
                                                                     cellStart, records, cutMasks, gridA, gridF);
@@ -2133,7 +2136,13 @@ namespace crb200
                                                           (recompute || adjReplay) ? adjTorque : ct);
                     CRB_LAUNCHED(2);
                 }
-            if (Multi || det == 0)
+            if constexpr (Multi)
+                if (det == 2) // the tiles in a fixed order; the coupling of dynamic shapes stays atomic
+                {
+                    upd(std::integral_constant<int, 2>{});
+                    CRB_LAUNCHED(1);
+                }
+            if (det == 0)
             {
                 upd(std::integral_constant<int, 0>{});
                 CRB_LAUNCHED(1);
@@ -2515,13 +2524,13 @@ namespace crb200
         }
         const unsigned g = (n + 127) / 128;
         const SceneTable sc = sceneTable();
-        if (detP2G && detFixedMass && !isBatch())
+        if (detP2G && detFixedMass)
         {
             unsigned *maxBits = reinterpret_cast<unsigned *>(detFixedMass + (size_t)totalBlocks * 64u);
             CRB_CHECK(cudaMemsetAsync(maxBits, 0, sizeof(unsigned), stream));
             k_initMaxMass<<<g, 128, 0, stream>>>(n, indices, positionMass, maxBits);
-            k_initMassFixed<<<g, 128, 0, stream>>>(geom, n, indices, positionMass, F, (unsigned)numMaxParticles, maxBits,
-                                                   detFixedMass);
+            k_initMassFixed<<<g, 128, 0, stream>>>(geom, sc, n, indices, positionMass, F, (unsigned)numMaxParticles,
+                                                   maxBits, detFixedMass);
             const unsigned nodes = totalBlocks * 64u;
             k_initMassFlush<<<(nodes + 255) / 256, 256, 0, stream>>>(nodes, maxBits, detFixedMass, gridA);
             CRB_LAUNCHED(3);

@@ -279,8 +279,10 @@ CRB200_API int CrB200SolverClearStatus(CrB200SolverHandle solver);
  * node tile (3.4 KB per grid block, allocated at the first switch-on) and the grid update sums the
  * tiles covering a node in a fixed order (the reference sums with float atomics in arrival order,
  * math_helpers.h:309-328).  Particles whose stencil leaves the grid still go through atomics.
- * Single-scene solvers only.  The substeps an adjoint backward pass replays follow the option, so a
- * recording made with it on is replayed bit for bit. */
+ * On a batch solver the particle state becomes reproducible the same way, while the coupling force
+ * and torque of dynamic shapes keep their float atomics (the fixed-order coupling reduction is for
+ * single scenes).  The substeps an adjoint backward pass replays follow the option, so a recording
+ * made with it on is replayed bit for bit. */
 #define CRB200_OPT_DETERMINISTIC 5
 /* CRB200_OPT_RESIDENT (off by default; no counterpart in the reference, whose solvers keep the
  * particles in the caller's order): single-scene MLS-MPM solvers keep their own copy of the

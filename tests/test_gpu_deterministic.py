@@ -1,5 +1,6 @@
 """Deterministic substeps (CRB200_OPT_DETERMINISTIC): P2G stores whole block tiles and the grid
-update sums each node's tiles in a fixed order; the coupling momentum is reduced in a fixed order.
+update sums each node's tiles in a fixed order; the coupling momentum is reduced in a fixed order
+(single scenes; batches keep the coupling atomics and reproduce the particle state).
 Two runs from the same state must agree bit for bit (the ordinary path sums with float atomics in
 arrival order, as the reference does, and does not), and a deterministic run must stay within the
 parity tolerance of the ordinary run and of the FP64 oracle."""
@@ -71,10 +72,28 @@ def test_deterministic_mls_cube_matches_fp64_oracle():
     assert rel_pos_err(a["x"], o.state()["x"], sc.pos_mass[:, :3], sc.cell_size) <= 1e-4
 
 
-def test_deterministic_refused_on_batches():
-    b = cb.DeviceBatch(scenes.batched_scenes(num_scenes=2, nmin=1000, nmax=2000))
-    with pytest.raises(cb.CrmpmError, match="batch"):
+def _batch_run(sl, steps, det):
+    b = cb.DeviceBatch(sl, compute_initial=False)
+    if det:
         b.solver.set_option(cb.OPT_DETERMINISTIC, 1)
+    b.compute_initial_data()
+    b.step(steps)
+    return b, b.state()
+
+
+def test_deterministic_batch_repeats_bit_for_bit():
+    """A batch in deterministic mode: two runs give the same particle state bit for bit, and each
+    scene stays within the parity tolerance of the ordinary (atomic) batch run."""
+    sl = scenes.batched_scenes(num_scenes=8, nmin=2000, nmax=8000)
+    steps = 60
+    b1, a = _batch_run(sl, steps, True)
+    _, c = _batch_run(sl, steps, True)
+    for k in ("x", "v", "F", "C"):
+        np.testing.assert_array_equal(a[k], c[k], err_msg=f"batch {k} differs between two deterministic runs")
+    _, o = _batch_run(sl, steps, False)
+    for s, sc in enumerate(sl):
+        got, ref = b1.scene_state(s, a), b1.scene_state(s, o)
+        assert rel_pos_err(got["x"], ref["x"], sc.pos_mass[:, :3], sc.cell_size) <= 1e-4, f"scene {s}"
 
 
 @pytest.mark.parametrize("case", ["mls_cube", "dynamic_sphere"])
