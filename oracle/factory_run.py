@@ -5,14 +5,16 @@ of every frame (CrAdvance + CrFetchResults, the scene's own readback included).
 
 Each build exports the same C symbols, so every run is its own process:
 
-    python oracle/factory_run.py LIB SCENE FRAMES OUT.npz [SPARE]
+    python oracle/factory_run.py LIB SCENE FRAMES OUT.npz [SPARE] [--cpu]
 
 SCENE: cube_mls, cube_pb, cube_standard (a 0.1 m Neo-Hookean cube dropped on a ground plane) or
 slab (the 1.0 x 0.2 x 1.0 m tissue slab, dx 0.01, particle spacing 0.005: about 1.6M particles,
 the four side faces held by static boxes, a kinematic sphere probe moving down at 0.1 m/s).
 Particles come from the reference's own particle-object sampler (a lattice inside the geometry,
 particle_object_impl.cpp:36-86).  SPARE (default 1.0): numMaxParticles of the scene as a multiple of
-the particles the object adds, to show what a scene's readback of numMaxParticles costs.
+the particles the object adds, to show what a scene's readback of numMaxParticles costs.  --cpu:
+the factory builds no GPU data, so every scene falls back to the reference's CPU solvers
+(simulation_factory_impl.cpp:351-378); it runs without a GPU.
 """
 import ctypes as C
 import sys
@@ -147,12 +149,14 @@ def build(lib, scene, spare):
 
 
 def main():
-    path, scene, frames, out = sys.argv[1], sys.argv[2], int(sys.argv[3]), sys.argv[4]
-    spare = float(sys.argv[5]) if len(sys.argv) > 5 else 1.0
+    args = [a for a in sys.argv[1:] if a != "--cpu"]
+    gpu = "--cpu" not in sys.argv[1:]
+    path, scene, frames, out = args[0], args[1], int(args[2]), args[3]
+    spare = float(args[4]) if len(args) > 4 else 1.0
     lib = _bind(C.CDLL(path))
     substeps = 10
     probe_n = 2_000_000 if scene == "slab" else 200_000
-    lib.CrInitializeEngine(int(probe_n * max(spare, 1.0)) + 1024, 64, 64, 1024, 1, 1)
+    lib.CrInitializeEngine(int(probe_n * max(spare, 1.0)) + 1024, 64, 64, 1024, 1 if gpu else 0, 1)
     if lib.CrGetInitializationStatus() == 0:
         raise SystemExit("CrInitializeEngine failed")
     sc, shapes, n, nmax, dt = build(lib, scene, spare)

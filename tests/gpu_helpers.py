@@ -1,4 +1,4 @@
-"""Helpers shared by the GPU parity tests."""
+"""Helpers shared by the parity tests."""
 import numpy as np
 
 
@@ -27,3 +27,21 @@ def canonical_permutation(keys, active):
     ids = np.nonzero(active)[0]
     order = np.lexsort((ids, keys[ids]))
     return ids[order].astype(np.uint32)
+
+
+def factory_oracle_scene(scene, x0):
+    """The factory cube (oracle/factory_run.py) as a scene for the FP64 oracle, from the particles
+    the reference's sampler made."""
+    from crmpm_b200 import scenes
+
+    n = x0.shape[0]
+    lam, mu = scenes.lame(1e4, 0.3)
+    mp = np.tile(np.array([lam, mu, 0, 0] if scene != "cube_pb" else [1.0, 0.9, 0, 0], np.float32), (n, 1))
+    st = scenes.ShapeTable.empty()
+    g = st.add_geometry(scenes.GEOM_PLANE, (0, 0, 0, 0))
+    st.add_shape(g, scenes.SHAPE_STATIC, (0, 0, 0), smooth=0.0, drag=1.0, friction=0.3)
+    solver = {"cube_mls": scenes.SOLVER_MLS, "cube_pb": scenes.SOLVER_PB, "cube_standard": scenes.SOLVER_STANDARD}[scene]
+    return scenes.Scene(solver, np.array([-0.3, -0.1, -0.3], np.float32), np.array([0.3, 0.4, 0.3], np.float32), 0.01,
+                        2e-4, np.array([0.05, -9.81, 0.03], np.float32), 10, 0, x0.astype(np.float32),
+                        np.zeros((n, 4), np.float32), mp, np.full(n, scenes.MAT_NEOHOOKEAN, np.int32),
+                        np.ones(n, np.uint8), st, "factory_" + scene)

@@ -19,6 +19,7 @@ import numpy as np
 import pytest
 
 from conftest import cuda_available
+from gpu_helpers import factory_oracle_scene
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not cuda_available(), reason="needs a CUDA GPU")]
 
@@ -55,24 +56,6 @@ def _compare(a, b, tol, what):
     assert ec <= 1e-3, f"{what}: coupling {ec:.3e}"
 
 
-def _oracle_scene(scene, x0):
-    """The factory cube (oracle/factory_run.py) as a scene for the FP64 oracle, from the particles
-    the reference's sampler made."""
-    from crmpm_b200 import scenes
-
-    n = x0.shape[0]
-    lam, mu = scenes.lame(1e4, 0.3)
-    mp = np.tile(np.array([lam, mu, 0, 0] if scene != "cube_pb" else [1.0, 0.9, 0, 0], np.float32), (n, 1))
-    st = scenes.ShapeTable.empty()
-    g = st.add_geometry(scenes.GEOM_PLANE, (0, 0, 0, 0))
-    st.add_shape(g, scenes.SHAPE_STATIC, (0, 0, 0), smooth=0.0, drag=1.0, friction=0.3)
-    solver = {"cube_mls": scenes.SOLVER_MLS, "cube_pb": scenes.SOLVER_PB, "cube_standard": scenes.SOLVER_STANDARD}[scene]
-    return scenes.Scene(solver, np.array([-0.3, -0.1, -0.3], np.float32), np.array([0.3, 0.4, 0.3], np.float32), 0.01,
-                        2e-4, np.array([0.05, -9.81, 0.03], np.float32), 10, 0, x0.astype(np.float32),
-                        np.zeros((n, 4), np.float32), mp, np.full(n, scenes.MAT_NEOHOOKEAN, np.int32),
-                        np.ones(n, np.uint8), st, "factory_" + scene)
-
-
 @pytest.mark.skipif(not built, reason="oracle/_ref/factory not built (make -C oracle ref-factory)")
 @pytest.mark.parametrize("scene,frames,tol", [("cube_mls", 40, 1e-4), ("cube_standard", 40, 1e-4), ("cube_pb", 40, 2e-3)])
 def test_factory_cube_through_the_c_api(scene, frames, tol, tmp_path):
@@ -88,7 +71,7 @@ def test_factory_cube_through_the_c_api(scene, frames, tol, tmp_path):
     ref = _run("ref", scene, frames, tmp_path)
     got = _run("b200", scene, frames, tmp_path)
     assert float(np.abs(ref["x"][:, :3] - ref["x0"][:, :3]).max()) > 1e-3, "the cube did not move"
-    sc = _oracle_scene(scene, ref["x0"])
+    sc = factory_oracle_scene(scene, ref["x0"])
     steps = frames * int(got["substeps"])
     o = op.PortOracle(sc, 64)
     o.compute_initial_data()
