@@ -1034,6 +1034,20 @@ namespace crb200
         const GridGeom &g = p.g;
         const ShapeRec *shp = Multi ? shapeTable + p.shapeBegin : sh;
         const bool slicers = Mode != 2 && p.numShapes > 0 && (sc.flags[si] & SF_SLICER);
+        // F (and for the next record the material and V0) are used only after the node gathers:
+        // start their DRAM reads into L2 now, so that they arrive while the gathers wait, without
+        // holding registers across them
+        if (Mode != 1)
+        {
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F + (size_t)e * stride + i));
+            if (Mode == 0 && records != nullptr)
+            {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(matParams + i));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(V0 + i));
+            }
+        }
         const float4 x4 = xm[i];
         const V3 x = v3(x4);
         const Stencil st = stencilOf(g, x);
